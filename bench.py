@@ -1,0 +1,406 @@
+"""Benchmark of the surfacelet analyze/synthesize path on B200.
+
+Workload (one step, per rank): NSSurfacelet(scales = 3, direction_levels =
+[2, 2, 3]) on a batch of float32 128^3 volumes, i.i.d. N(0, 1) from a seeded
+generator: analyze, synthesize, and the adjoint of synthesize, per volume.
+Metric: Mvoxels/s of input volume through analyze + synthesize + adjoint,
+whole job (all ranks).  Each volume's coefficients are 411 MB, larger than
+the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl reference]
+
+Under torchrun (N > 1) each rank runs its own batch (weak scaling, no
+data-path collective); the elapsed time is the max over ranks.  The line
+also carries: e2e (the same step through the public API with pinned host
+buffers, copies inside the timed region), the roofline of the dominant kernel
+(CUDA-event launch times from a profiled replay), the float64-oracle CPU
+baseline, the plain unfused GPU form (cuFFT through torch, timing comparison
+only), and the decimated Surfacelet 128^3 line as `secondary`.
+"""
+
+import argparse
+import datetime
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "Mvoxels/s analyze+synthesize(+adjoint), fused vs plain GPU at rel.err ≤1e-5"
+DIMS = (128, 128, 128)
+NS_KW = dict(scales=3, direction_levels=[2, 2, 3])
+DEC_KW = dict(scales=3, direction_levels=[2, 2, 3], pyramid_ratio=2)
+
+
+def load_package():
+    name = "surfacelets_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "surfacelets.jl_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ── clocks during the timed region ──────────────────────────────────────────
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        if not sm:
+            return None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ── the reference arm: the oracle port on the host cores ────────────────────
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, ROOT)
+    from oracle import ns as N
+    from oracle.cpu_baseline import NSBaseline
+    cores = os.cpu_count()
+    base = NSBaseline(N.NSParams.make(**NS_KW), DIMS, np.float32, workers=cores)
+    x = np.random.default_rng(0).standard_normal(DIMS).astype(np.float32)
+
+    def step():
+        c = base.analyze(x)
+        y = base.synthesize(c)
+        base.analyze(y, synth_masks=True)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    v = float(np.prod(DIMS)) / dt / 1e6
+    line = {
+        "metric": METRIC, "value": v, "unit": "Mvoxels/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "NSSurfacelet(scales=3, direction_levels=[2,2,3]) 128^3 float32, "
+                               "analyze+synthesize+adjoint of one volume per step", "batch": 1},
+        "cpu_baseline": {"value": v, "unit": "Mvoxels/s", "cores": cores, "kind": "port",
+                         "sample": "one 128^3 volume analyze+synthesize+adjoint per step, scipy.fft "
+                                   f"with workers={cores}, float32 masks from the float64 oracle"},
+        "e2e": {"value": v, "unit": "Mvoxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ── our arm ──────────────────────────────────────────────────────────────────
+
+
+def kernel_bytes(tag, P, launches_per_step, nz_total):
+    """Algorithmic bytes of all launches of `tag` in one profiled step: each
+    input read once and each output written once (float32 volumes: 4 B a
+    voxel; spectra on the rfft grid: 8 B a bin)."""
+    N = float(np.prod(DIMS))
+    H = float((DIMS[0] // 2 + 1) * DIMS[1] * DIMS[2])
+    per_item = {
+        "ns_r2c_axis1": 4 * N + 8 * H,
+        "ns_c2r_axis1": 8 * H + 4 * N,
+        "ns_c2c_axis2": 16 * H,
+        "ns_c2c_axis3": 16 * H,
+        "ns_mask_axis3": 8 * H,
+        "ns_accum_axis3": 8 * H,
+    }.get(tag)
+    if per_item is None:
+        return None
+    extra = {"ns_mask_axis3": 8 * H, "ns_accum_axis3": 32 * H}.get(tag, 0.0)
+    return per_item * nz_total + extra * launches_per_step
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip plain/secondary/cpu legs")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    sfl = load_package()
+    B = args.batch
+    N = int(np.prod(DIMS))
+    t = sfl.NSSurfacelet(**NS_KW)
+    ws = sfl.make_workspace(t, "float32", DIMS)
+    S = ws.nsubbands
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    xs = [sfl.volume_like(DIMS).copy_(torch.randn(DIMS, device="cuda", generator=gen)) for _ in range(B)]
+    cs = [sfl.volume_like(DIMS + (S,)) for _ in range(B)]
+    gs = [sfl.volume_like(DIMS + (S,)) for _ in range(B)]
+    ys = [sfl.volume_like(DIMS) for _ in range(B)]
+
+    def step():
+        for b in range(B):
+            sfl.analyze_(cs[b], ws, xs[b])
+            sfl.synthesize_(ys[b], ws, cs[b])
+            sfl.adjoint_synthesize_(gs[b], ws, ys[b])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            v = torch.tensor([ms], device="cuda")
+            dist.all_reduce(v, op=dist.ReduceOp.MAX)
+            ms = float(v.item())
+        return ms
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    ms = timed(step, args.steps)
+    clk = clocks.stop() if clocks else None
+    value = B * N * world / (ms / 1e3) / 1e6
+
+    # correctness of the timed data: perfect reconstruction and A^T = A (tight)
+    rel_pr = max(float(torch.linalg.vector_norm(ys[b] - xs[b]) / torch.linalg.vector_norm(xs[b])) for b in range(B))
+    rel_adj = float(torch.linalg.vector_norm(gs[0] - cs[0]) / torch.linalg.vector_norm(cs[0]))
+
+    # profiled replay: launch counts and per-kernel CUDA-event times
+    lib = sfl.lib
+    lib.sfl_profile_reset()
+    lib.sfl_profile_enable(1)
+    prof_steps = 2
+    for _ in range(prof_steps):
+        step()
+    torch.cuda.synchronize()
+    lib.sfl_profile_enable(0)
+    import ctypes as C
+    buf = C.create_string_buffer(4096)
+    lib.sfl_profile_tags(buf, 4096)
+    tags = [s for s in buf.value.decode().split("\n") if s]
+    per_tag = {}
+    for tg in tags:
+        tot, cnt = C.c_double(), C.c_int64()
+        lib.sfl_profile_read(tg.encode(), C.byref(tot), C.byref(cnt))
+        per_tag[tg] = (tot.value / prof_steps, cnt.value // prof_steps)
+    lib.sfl_profile_reset()
+    launches_per_step = sum(c for _, c in per_tag.values())
+    dom = max(per_tag, key=lambda k: per_tag[k][0])
+    dom_ms, dom_launches = per_tag[dom]
+    # items processed per step by the dominant kernel (sum of grid.y over its launches)
+    # spectra/volumes each kernel tag processes per step (grid.y summed over its launches):
+    # analyze = rfft3 + per subband (mask pass, axis-2 pass, C2R); synthesize = per subband
+    # (R2C, axis-2 pass, accumulation) + irfft3; the adjoint of synthesize is an analysis.
+    nz_total = {
+        "ns_r2c_axis1": B * (S + 2), "ns_c2r_axis1": B * (2 * S + 1), "ns_c2c_axis2": B * (3 * S + 3),
+        "ns_c2c_axis3": B * 3, "ns_mask_axis3": B * 2 * S, "ns_accum_axis3": B * S,
+    }.get(dom, 0)
+    hbm, peak_kind = peaks()
+    alg = kernel_bytes(dom, None, dom_launches, nz_total)
+    achieved = alg / (dom_ms / 1e3) / 1e9 if alg else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        tj = json.load(open(tfile)).get(dom)
+        if tj:
+            traffic = tj.get("bytes_per_launch_full_size")
+    op_bytes = 600.0 * N * B * world     # 4(1+S)*3 B a voxel at S = 49
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mvoxels/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "NSSurfacelet(scales=3, direction_levels=[2,2,3]) 128^3 float32, "
+                               "analyze+synthesize+adjoint(synthesize) per volume",
+                   "batch_per_gpu": B, "global_batch": B * world, "volume": list(DIMS),
+                   "parallelism": f"replicas x{world} (no collective)",
+                   "l2": "inputs larger than L2 (411 MB of coefficients a volume)"},
+        "gpu_launches": launches_per_step * args.steps,
+        "rel_err": {"perfect_reconstruction_rel_l2": rel_pr, "adjoint_vs_analyze_rel_l2": rel_adj},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "launches_per_step": dom_launches, "ms_per_step": dom_ms,
+                     "share_of_step": dom_ms / ms},
+        "op_roofline": {"algorithmic_bytes_per_voxel": 600, "achieved_gbs": op_bytes / (ms / 1e3) / 1e9 / world,
+                        "frac": op_bytes / (ms / 1e3) / 1e9 / world / hbm, "peak_kind": peak_kind},
+        "kernel_ms_per_step": {k: v[0] for k, v in per_tag.items()},
+    }
+    if clk:
+        line["clocks"] = {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}
+
+    # e2e: public API with pinned host buffers, copies inside the timed region
+    hx = [torch.empty(DIMS[::-1], dtype=torch.float32).pin_memory() for _ in range(B)]
+    hy = [torch.empty(DIMS[::-1], dtype=torch.float32).pin_memory() for _ in range(B)]
+    for b in range(B):
+        hx[b].copy_(xs[b].permute(2, 1, 0))
+    dx = [sfl.volume_like(DIMS) for _ in range(B)]
+
+    def e2e_step():
+        for b in range(B):
+            dx[b].permute(2, 1, 0).copy_(hx[b], non_blocking=True)
+            sfl.analyze_(cs[b], ws, dx[b])
+            sfl.synthesize_(ys[b], ws, cs[b])
+            sfl.adjoint_synthesize_(gs[b], ws, ys[b])
+            hy[b].copy_(ys[b].permute(2, 1, 0), non_blocking=True)
+
+    e2e_step()
+    ms_e2e = timed(e2e_step, max(3, args.steps // 2))
+    line["e2e"] = {"value": B * N * world / (ms_e2e / 1e3) / 1e6, "unit": "Mvoxels/s",
+                   "h2d_bytes_per_step": 4 * N * B, "d2h_bytes_per_step": 4 * N * B}
+
+    if not args.no_extras and rank == 0:
+        # plain unfused single-volume GPU form: the reference's device path
+        # (materialized masks, one cuFFT call per subband) through torch.fft
+        sys.path.insert(0, ROOT)
+        from oracle import ns as ON
+        T = ON.make_tables(ON.NSParams.make(**NS_KW), DIMS)
+        masks = [(s, torch.from_numpy(M.astype(np.float32).transpose().copy()).cuda())
+                 for s, M in ON.subband_masks(T, analysis=True)]
+        xt = xs[0].permute(2, 1, 0)       # C-order (n3, n2, n1): the rfft axis is last
+
+        def plain_step():
+            X = torch.fft.rfftn(xt)
+            cpl = [None] * S
+            for s, M in masks:
+                cpl[s - 1] = torch.fft.irfftn(X * M, s=xt.shape)
+            acc = None
+            for s, M in masks:
+                F = torch.fft.rfftn(cpl[s - 1]) * M
+                acc = F if acc is None else acc + F
+            y = torch.fft.irfftn(acc, s=xt.shape)
+            X2 = torch.fft.rfftn(y)
+            for s, M in masks:
+                torch.fft.irfftn(X2 * M, s=xt.shape)
+
+        for _ in range(2):
+            plain_step()
+        ms_plain = timed(plain_step, 3)
+        plain = N / (ms_plain / 1e3) / 1e6
+        line["plain_gpu"] = {"value": plain, "unit": "Mvoxels/s",
+                             "form": "torch.fft (cuFFT) + materialized masks, one volume, unfused",
+                             "fused_over_plain_per_volume": (value / world) / plain}
+        del masks
+        torch.cuda.empty_cache()
+
+        # secondary line: the decimated Surfacelet at 128^3 (pyramid_ratio 2)
+        u = sfl.Surfacelet(**DEC_KW)
+        wd = sfl.make_workspace(u, "float32", DIMS)
+        cd = torch.empty(wd.ncoeffs, device="cuda")
+        yd = sfl.volume_like(DIMS)
+
+        def dec_step():
+            for b in range(B):
+                sfl.analyze_(cd, wd, xs[b])
+                sfl.synthesize_(yd, wd, cd)
+
+        for _ in range(3):
+            dec_step()
+        ms_dec = timed(dec_step, max(3, args.steps // 2))
+        rel_dec = float(torch.linalg.vector_norm(yd - xs[B - 1]) / torch.linalg.vector_norm(xs[B - 1]))
+        line["secondary"] = {"workload": "Surfacelet(scales=3, direction_levels=[2,2,3], pyramid_ratio=2) "
+                                         "128^3 float32, analyze+synthesize",
+                             "value": B * N / (ms_dec / 1e3) / 1e6, "unit": "Mvoxels/s",
+                             "perfect_reconstruction_rel_l2": rel_dec,
+                             "algorithmic_bytes_per_voxel": 4 * 2 * (1 + wd.ncoeffs / N)}
+
+        # CPU baseline: the oracle port on the host cores, bounded sample
+        from oracle.cpu_baseline import NSBaseline
+        cores = os.cpu_count()
+        base = NSBaseline(ON.NSParams.make(**NS_KW), DIMS, np.float32, workers=cores)
+        xh = xs[0].permute(2, 1, 0).cpu().numpy().transpose()
+        reps = 2
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            cb = base.analyze(xh)
+            yb = base.synthesize(cb)
+            base.analyze(yb, synth_masks=True)
+        dt = (time.perf_counter() - t0) / reps
+        line["cpu_baseline"] = {"value": N / dt / 1e6, "unit": "Mvoxels/s", "cores": cores, "kind": "port",
+                                "sample": f"{reps} x (analyze+synthesize+adjoint) of one 128^3 volume, "
+                                          f"scipy.fft workers={cores}, float32"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,220 @@
+/*
+ * surfacelets_b200 — C ABI of the B200 (sm_100a) surfacelet analyze/synthesize
+ * library.
+ *
+ * This is the drop-in boundary for the device path of hakkelt/Surfacelets.jl.
+ * Each entry point below replaces one method of the reference's
+ * AbstractMultiscaleTransforms interface for `NSSurfacelet` and the decimated
+ * `Surfacelet`; the citation in front of each declaration names the reference
+ * method (file:line in the Surfacelets.jl tree) whose behaviour it takes over.
+ *
+ * Conventions
+ *   - Every function returns an int status: SFL_OK (0) or a negative code.
+ *     SFL_ERR_ARGUMENT maps to Julia's ArgumentError and SFL_ERR_DIMENSION to
+ *     DimensionMismatch; sfl_last_error() holds the message (thread-local), in
+ *     the reference's own wording.
+ *   - Volumes are column-major (axis 1 fastest), real float32 or complex
+ *     float32 with interleaved real/imaginary parts.  Complex data runs as two
+ *     real channels through the same kernels, so the transform is exactly
+ *     real-linear (bit for bit).
+ *   - NSSurfacelet coefficients are one (n1, n2, n3, S) array: subband i
+ *     (1-based, lowpass first) is the contiguous volume at element offset
+ *     (i-1)*n1*n2*n3.  Surfacelet coefficients are one flat vector with each
+ *     subband a contiguous column-major block at the offset sfl_subband_info
+ *     reports (the reference's SubbandVector).
+ *   - Data pointers passed to sfl_analyze & co. are device pointers; `stream`
+ *     is a cudaStream_t (NULL = the legacy default stream).  Calls are
+ *     asynchronous with respect to the host unless stated otherwise.
+ *   - A plan owns its tables and scratch.  It is not reentrant: one call at a
+ *     time per plan (the reference's workspaces have the same rule,
+ *     src/transforms/ns_surfacelet.jl:51-53, src/transforms/surfacelet.jl:40-44).
+ */
+#ifndef SURFACELETS_B200_H
+#define SURFACELETS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFL_OK 0
+#define SFL_DONE 1               /* a stream has no further subband */
+#define SFL_ERR_ARGUMENT (-1)    /* ArgumentError */
+#define SFL_ERR_DIMENSION (-2)   /* DimensionMismatch */
+#define SFL_ERR_CUDA (-3)        /* a CUDA call failed */
+#define SFL_ERR_ALLOC (-4)       /* device memory could not be allocated */
+#define SFL_ERR_STATE (-5)       /* call out of order (streaming) */
+#define SFL_ERR_UNSUPPORTED (-6) /* a size or option this build does not handle */
+
+#define SFL_MAX_SCALES 16
+
+#define SFL_REAL32 0
+#define SFL_COMPLEX64 1
+
+#define SFL_KIND_NS 0
+#define SFL_KIND_DECIMATED 1
+
+/* NSSurfacelet(; scales, direction_levels, bernstein_order, halfband_order,
+ *              transition, tight) — src/types/transforms.jl:86-113.
+ * direction_levels[j] for j = 0 .. scales-1, coarsest scale first. */
+typedef struct {
+    int32_t scales;
+    int32_t direction_levels[SFL_MAX_SCALES];
+    int32_t bernstein_order;
+    int32_t halfband_order;
+    double transition;
+    int32_t tight;
+} sfl_ns_params;
+
+/* Surfacelet(; scales, direction_levels, pyramid_ratio, checkerboard_order,
+ *            diamond_length, kaiser_beta, diamond_power) —
+ * src/types/transforms.jl:222-261.  levels[j][K][m] is the level matrix of
+ * scale j (coarsest first): the number of checkerboard stages along axis m
+ * inside hourglass K (diagonal ignored).  Integer levels convert with
+ * sfl_surf_levels_from_int. */
+typedef struct {
+    int32_t scales;
+    int32_t levels[SFL_MAX_SCALES][3][3];
+    double pyramid_ratio;
+    int32_t checkerboard_order;
+    int32_t diamond_length;
+    double kaiser_beta;
+    int32_t diamond_power;
+} sfl_surf_params;
+
+typedef struct sfl_plan sfl_plan;
+
+/* Message of the last failed call on this thread ("" when none). */
+const char* sfl_last_error(void);
+
+/* Library version string. */
+const char* sfl_version(void);
+
+/* ── Parameter and layout queries (host only, no device needed) ─────────── */
+
+/* Constructor validation of NSSurfacelet: src/types/transforms.jl:93-104. */
+int sfl_ns_check_params(const sfl_ns_params* p);
+
+/* Size validation of make_workspace, including the empty-scale refusal:
+ * src/transforms/ns_surfacelet.jl:98-115. */
+int sfl_ns_check_size(const sfl_ns_params* p, const int32_t dims[3]);
+
+/* nsubbands(t, dims): src/transforms/ns_surfacelet.jl:527. */
+int sfl_ns_nsubbands(const sfl_ns_params* p, int32_t* n);
+
+/* subband_layout(t, dims): (scale, direction) per subband, lowpass (0, 0)
+ * first; arrays of nsubbands entries.  src/transforms/ns_surfacelet.jl:518-525. */
+int sfl_ns_layout(const sfl_ns_params* p, int32_t* scale, int32_t* direction);
+
+/* Integer directional level L to a level matrix: src/types/transforms.jl:270-278. */
+int sfl_surf_levels_from_int(int32_t L, int32_t out[3][3]);
+
+/* Constructor validation of Surfacelet: src/types/transforms.jl:231-251. */
+int sfl_surf_check_params(const sfl_surf_params* p);
+
+/* Subband sizes and layout, with the reference's size validation
+ * (src/transforms/surfacelet.jl:230-308).  *n receives the subband count;
+ * sizes (3 per subband), scale, hourglass and wedge may be NULL. */
+int sfl_surf_layout(const sfl_surf_params* p, const int32_t dims[3], int32_t* n,
+                    int32_t* sizes, int32_t* scale, int32_t* hourglass, int32_t* wedge);
+
+/* surfacelet_redundancy(t, dims): src/transforms/surfacelet.jl:220-222. */
+int sfl_surf_redundancy(const sfl_surf_params* p, const int32_t dims[3], double* r);
+
+/* ── Plans (make_workspace) ─────────────────────────────────────────────── */
+
+/* make_workspace(t::NSSurfacelet, T, dims): src/transforms/ns_surfacelet.jl:88-123.
+ * Designs the masks in float64, stores them as float32 on the current device
+ * and allocates the scratch.  dtype is SFL_REAL32 or SFL_COMPLEX64. */
+int sfl_ns_plan_create(const sfl_ns_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out);
+
+/* make_workspace(t::Surfacelet, T, dims): src/transforms/surfacelet.jl:126-149. */
+int sfl_surf_plan_create(const sfl_surf_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out);
+
+/* Releases a plan and its device memory (synchronizes the device first). */
+int sfl_plan_destroy(sfl_plan* plan);
+
+/* transform(ws), size(ws), eltype(ws), nsubbands, coefficient count:
+ * src/transforms/ns_surfacelet.jl:78-80, src/transforms/surfacelet.jl:63-65. */
+int sfl_plan_info(const sfl_plan* plan, int32_t* kind, int32_t dims[3], int32_t* dtype,
+                  int32_t* nsubbands, int64_t* ncoeffs);
+
+/* subband(t, c, i): shape of subband i (1-based) and its element offset in
+ * the coefficients.  src/transforms/ns_surfacelet.jl:539,
+ * src/transforms/surfacelet.jl:444. */
+int sfl_subband_info(const sfl_plan* plan, int32_t i, int32_t shape[3], int64_t* offset);
+
+/* Subbands a launch keeps in flight (NS: scratch holds that many spectra).
+ * Default 8; only affects speed and scratch size. */
+int sfl_plan_set_group(sfl_plan* plan, int32_t group);
+
+/* ── Transforms ─────────────────────────────────────────────────────────── */
+
+/* analyze!(c, t, x; workspace): src/transforms/ns_surfacelet.jl:551-566,
+ * src/transforms/surfacelet.jl:446-454. */
+int sfl_analyze(sfl_plan* plan, const void* x, void* c, void* stream);
+
+/* synthesize!(x, t, c; workspace): src/transforms/ns_surfacelet.jl:568-581,
+ * src/transforms/surfacelet.jl:456-464. */
+int sfl_synthesize(sfl_plan* plan, const void* c, void* x, void* stream);
+
+/* Adjoint of analyze (x = A^T c).  The reference has no adjoint entry point:
+ * for a tight NSSurfacelet the inverse is the adjoint
+ * (src/transforms/ns_surfacelet.jl:21-25) and this equals sfl_synthesize;
+ * otherwise (tight = false, and the decimated transform, whose checkerboard
+ * filters are biorthogonal, src/transforms/surfacelet.jl:24-26) it applies
+ * the transposed analysis operator. */
+int sfl_adjoint_analyze(sfl_plan* plan, const void* c, void* x, void* stream);
+
+/* Adjoint of synthesize (c = S^T x); equals sfl_analyze for a tight NSSurfacelet. */
+int sfl_adjoint_synthesize(sfl_plan* plan, const void* x, void* c, void* stream);
+
+/* ── Streaming (NSSurfacelet only) ─────────────────────────────────────── */
+
+/* Streaming analyze(f, t, x): src/transforms/ns_surfacelet.jl:474-479, 620-624.
+ * begin transforms x once; each next writes the next subband (a volume of
+ * the plan's dims and element type) to `band` and its 1-based index to
+ * *index, in the reference's order: the directional subbands in increasing
+ * index, then the lowpass (index 1).  next returns SFL_DONE after the last. */
+int sfl_stream_analyze_begin(sfl_plan* plan, const void* x, void* stream);
+int sfl_stream_analyze_next(sfl_plan* plan, void* band, int32_t* index, void* stream);
+
+/* Streaming synthesize!(f, x, t): src/transforms/ns_surfacelet.jl:483-500,
+ * 626-641.  next_index tells which subband the plan wants next (same order as
+ * analysis; SFL_DONE when all were pushed); push consumes it; end writes x. */
+int sfl_stream_synthesize_begin(sfl_plan* plan, void* stream);
+int sfl_stream_synthesize_next_index(sfl_plan* plan, int32_t* index);
+int sfl_stream_synthesize_push(sfl_plan* plan, const void* band, void* stream);
+int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream);
+
+/* ── Design tables (host only; for tests and inspection) ──────────────────
+ * Writes the float64 design table `name` (index selects one of several) of a
+ * transform on `dims` to out (when not NULL) and its element count to *count.
+ * Names (NS): "m1", "m2", "wedge" (index = ((scale-1)*3 + hourglass-1)*64*2
+ * + plane*64 + wedge-1, plane 0 = a, 1 = b), "pa" (index = level*3 + axis),
+ * "pl" (same).  Names (decimated): "ritf" (index = level*3 + K-1),
+ * "irc" (complex as re/im pairs; index = ((level*3 + K-1)*32 + stage)*4 + which,
+ * which 0,1 = analysis channel 0,1 and 2,3 = synthesis channel 0,1),
+ * "pyr_prof" (index = level*3 + axis).  No counterpart in the reference's
+ * interface: it exposes the internal tables of src/directional/*.jl. */
+int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const char* name,
+                        int32_t index, double* out, int64_t* count);
+int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name,
+                          int32_t index, double* out, int64_t* count);
+
+/* ── Launch timing (benchmark instrumentation) ───────────────────────────
+ * No counterpart in the reference.  While enabled, every kernel launch of the
+ * library is bracketed by two CUDA events on its stream and filed under its
+ * kernel tag; read sums the elapsed times of one tag (NULL = all), waiting
+ * for the events.  tags writes the newline-separated tag list to buf. */
+int sfl_profile_enable(int32_t on);
+int sfl_profile_reset(void);
+int sfl_profile_read(const char* tag, double* total_ms, int64_t* launches);
+int sfl_profile_tags(char* buf, int64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SURFACELETS_B200_H */

@@ -1,0 +1,556 @@
+// extern "C" entry points of libsurfacelets_b200.so (declared in
+// include/surfacelets_b200.h).  Every entry point catches the library's
+// exceptions and turns them into a status code plus a thread-local message.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "../../include/surfacelets_b200.h"
+#include "design.h"
+#include "plan.h"
+
+namespace sfl {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            throw AllocError(std::string(what) + ": " + cudaGetErrorString(e));
+        }
+        throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+DevMem::~DevMem() {
+    if (p) cudaFree(p);
+}
+
+void DevMem::alloc(size_t n) {
+    if (p) {
+        cudaFree(p);
+        p = nullptr;
+    }
+    bytes = n;
+    cuda_check(cudaMalloc(&p, n ? n : 1), "cudaMalloc");
+}
+
+}  // namespace sfl
+
+struct sfl_plan {
+    sfl::Plan impl;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        g_error.clear();
+        return f();
+    } catch (const sfl::ArgError& e) {
+        g_error = e.what();
+        return SFL_ERR_ARGUMENT;
+    } catch (const sfl::DimError& e) {
+        g_error = e.what();
+        return SFL_ERR_DIMENSION;
+    } catch (const sfl::AllocError& e) {
+        g_error = e.what();
+        return SFL_ERR_ALLOC;
+    } catch (const sfl::CudaError& e) {
+        g_error = e.what();
+        return SFL_ERR_CUDA;
+    } catch (const sfl::StateError& e) {
+        g_error = e.what();
+        return SFL_ERR_STATE;
+    } catch (const std::bad_alloc&) {
+        g_error = "host memory exhausted";
+        return SFL_ERR_ALLOC;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return SFL_ERR_ARGUMENT;
+    }
+}
+
+void need(const void* p, const char* what) {
+    if (!p) throw sfl::ArgError(std::string(what) + " must not be NULL");
+}
+
+void dims_of(const int32_t* d, int out[3]) {
+    need(d, "dims");
+    for (int i = 0; i < 3; ++i) out[i] = d[i];
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+void check_aligned(const void* p, int dtype, const char* what) {
+    uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    size_t need_al = dtype == SFL_COMPLEX64 ? 8 : 4;
+    if (a % need_al != 0)
+        throw sfl::ArgError(std::string(what) + " is not aligned to its element type");
+}
+
+// Runs f with the plan's device current, restoring the caller's afterwards.
+template <class F>
+void on_device(const sfl_plan* plan, F&& f) {
+    int cur = 0;
+    sfl::cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
+    if (cur != plan->impl.device) sfl::cuda_check(cudaSetDevice(plan->impl.device), "cudaSetDevice");
+    try {
+        f();
+    } catch (...) {
+        if (cur != plan->impl.device) cudaSetDevice(cur);
+        throw;
+    }
+    if (cur != plan->impl.device) sfl::cuda_check(cudaSetDevice(cur), "cudaSetDevice");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sfl_last_error(void) { return g_error.c_str(); }
+
+const char* sfl_version(void) { return "surfacelets_b200 0.1.0 (sm_100a)"; }
+
+int sfl_ns_check_params(const sfl_ns_params* p) {
+    return guarded([&] {
+        need(p, "params");
+        sfl::ns_check_params(*p);
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_check_size(const sfl_ns_params* p, const int32_t dims[3]) {
+    return guarded([&] {
+        need(p, "params");
+        int d[3];
+        dims_of(dims, d);
+        sfl::ns_check_params(*p);
+        sfl::ns_check_size(*p, d);
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_nsubbands(const sfl_ns_params* p, int32_t* n) {
+    return guarded([&] {
+        need(p, "params");
+        need(n, "n");
+        sfl::ns_check_params(*p);
+        *n = sfl::ns_nsubbands(*p);
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_layout(const sfl_ns_params* p, int32_t* scale, int32_t* direction) {
+    return guarded([&] {
+        need(p, "params");
+        sfl::ns_check_params(*p);
+        int k = 0;
+        if (scale) scale[k] = 0;
+        if (direction) direction[k] = 0;
+        ++k;
+        for (int j = 1; j <= p->scales; ++j)
+            for (int d = 1; d <= sfl::ns_nbands(*p, j); ++d, ++k) {
+                if (scale) scale[k] = j;
+                if (direction) direction[k] = d;
+            }
+        return SFL_OK;
+    });
+}
+
+int sfl_surf_levels_from_int(int32_t L, int32_t out[3][3]) {
+    return guarded([&] {
+        need(out, "out");
+        int o[3][3];
+        sfl::surf_levels_from_int(L, o);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) out[i][j] = o[i][j];
+        return SFL_OK;
+    });
+}
+
+int sfl_surf_check_params(const sfl_surf_params* p) {
+    return guarded([&] {
+        need(p, "params");
+        sfl::surf_check_params(*p);
+        return SFL_OK;
+    });
+}
+
+int sfl_surf_layout(const sfl_surf_params* p, const int32_t dims[3], int32_t* n, int32_t* sizes, int32_t* scale,
+                    int32_t* hourglass, int32_t* wedge) {
+    return guarded([&] {
+        need(p, "params");
+        int d[3];
+        dims_of(dims, d);
+        sfl::surf_check_params(*p);
+        auto sz = sfl::surf_layout_sizes(*p, d);
+        if (n) *n = (int32_t)sz.size();
+        if (sizes)
+            for (size_t i = 0; i < sz.size(); ++i)
+                for (int k = 0; k < 3; ++k) sizes[3 * i + k] = sz[i][k];
+        int k = 0;
+        if (scale) scale[0] = 0;
+        if (hourglass) hourglass[0] = 0;
+        if (wedge) wedge[0] = 0;
+        ++k;
+        for (int j = 1; j <= p->scales; ++j)
+            for (int K = 1; K <= 3; ++K) {
+                int s = 0;
+                for (int m = 0; m < 3; ++m)
+                    if (m != K - 1) s += p->levels[j - 1][K - 1][m];
+                for (int w = 1; w <= (1 << s); ++w, ++k) {
+                    if (scale) scale[k] = j;
+                    if (hourglass) hourglass[k] = K;
+                    if (wedge) wedge[k] = w;
+                }
+            }
+        return SFL_OK;
+    });
+}
+
+int sfl_surf_redundancy(const sfl_surf_params* p, const int32_t dims[3], double* r) {
+    return guarded([&] {
+        need(p, "params");
+        need(r, "r");
+        int d[3];
+        dims_of(dims, d);
+        sfl::surf_check_params(*p);
+        auto sz = sfl::surf_layout_sizes(*p, d);
+        double tot = 0;
+        for (auto& s : sz) tot += (double)s[0] * s[1] * s[2];
+        *r = tot / ((double)d[0] * d[1] * d[2]);
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_plan_create(const sfl_ns_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out) {
+    return guarded([&] {
+        need(p, "params");
+        need(out, "out");
+        *out = nullptr;
+        if (dtype != SFL_REAL32 && dtype != SFL_COMPLEX64) throw sfl::ArgError("dtype must be SFL_REAL32 or SFL_COMPLEX64");
+        int d[3];
+        dims_of(dims, d);
+        sfl::ns_check_params(*p);
+        sfl::ns_check_size(*p, d);
+        std::unique_ptr<sfl_plan> plan(new sfl_plan);
+        plan->impl.kind = SFL_KIND_NS;
+        plan->impl.dtype = dtype;
+        sfl::cuda_check(cudaGetDevice(&plan->impl.device), "cudaGetDevice");
+        plan->impl.ns.reset(new sfl::NSPlan);
+        sfl::ns_plan_init(*plan->impl.ns, *p, d, dtype);
+        *out = plan.release();
+        return SFL_OK;
+    });
+}
+
+int sfl_surf_plan_create(const sfl_surf_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out) {
+    return guarded([&] {
+        need(p, "params");
+        need(out, "out");
+        *out = nullptr;
+        if (dtype != SFL_REAL32 && dtype != SFL_COMPLEX64) throw sfl::ArgError("dtype must be SFL_REAL32 or SFL_COMPLEX64");
+        int d[3];
+        dims_of(dims, d);
+        sfl::surf_check_params(*p);
+        sfl::surf_layout_sizes(*p, d);
+        std::unique_ptr<sfl_plan> plan(new sfl_plan);
+        plan->impl.kind = SFL_KIND_DECIMATED;
+        plan->impl.dtype = dtype;
+        sfl::cuda_check(cudaGetDevice(&plan->impl.device), "cudaGetDevice");
+        sfl::dec_plan_create(plan->impl, *p, d, dtype);
+        *out = plan.release();
+        return SFL_OK;
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int sfl_plan_destroy(sfl_plan* plan) {
+    return guarded([&] {
+        if (!plan) return SFL_OK;
+        on_device(plan, [&] {
+            cudaDeviceSynchronize();
+            plan->impl.dec.reset();
+            plan->impl.ns.reset();
+        });
+        delete plan;
+        return SFL_OK;
+    });
+}
+
+int sfl_plan_info(const sfl_plan* plan, int32_t* kind, int32_t dims[3], int32_t* dtype, int32_t* nsubbands,
+                  int64_t* ncoeffs) {
+    return guarded([&] {
+        need(plan, "plan");
+        const sfl::Plan& P = plan->impl;
+        if (kind) *kind = P.kind;
+        if (dtype) *dtype = P.dtype;
+        if (P.kind == SFL_KIND_NS) {
+            const sfl::NSPlan& N = *P.ns;
+            if (dims)
+                for (int i = 0; i < 3; ++i) dims[i] = N.dims[i];
+            if (nsubbands) *nsubbands = N.S;
+            if (ncoeffs) *ncoeffs = N.N * N.S;
+        } else {
+            const sfl::SurfDesign& D = sfl::dec_design(*P.dec);
+            if (dims)
+                for (int i = 0; i < 3; ++i) dims[i] = D.dims[i];
+            if (nsubbands) *nsubbands = sfl::dec_nsubbands(*P.dec);
+            if (ncoeffs) *ncoeffs = sfl::dec_ncoeffs(*P.dec);
+        }
+        return SFL_OK;
+    });
+}
+
+int sfl_subband_info(const sfl_plan* plan, int32_t i, int32_t shape[3], int64_t* offset) {
+    return guarded([&] {
+        need(plan, "plan");
+        const sfl::Plan& P = plan->impl;
+        int n = P.kind == SFL_KIND_NS ? P.ns->S : sfl::dec_nsubbands(*P.dec);
+        if (i < 1 || i > n)
+            throw sfl::ArgError("subband index " + std::to_string(i) + " out of range 1:" + std::to_string(n));
+        int sh[3];
+        long long off;
+        if (P.kind == SFL_KIND_NS) {
+            for (int k = 0; k < 3; ++k) sh[k] = P.ns->dims[k];
+            off = (long long)(i - 1) * P.ns->N;
+        } else {
+            sfl::dec_subband_info(*P.dec, i, sh, &off);
+        }
+        if (shape)
+            for (int k = 0; k < 3; ++k) shape[k] = sh[k];
+        if (offset) *offset = off;
+        return SFL_OK;
+    });
+}
+
+int sfl_plan_set_group(sfl_plan* plan, int32_t group) {
+    return guarded([&] {
+        need(plan, "plan");
+        if (group < 1) throw sfl::ArgError("group must be ≥ 1, got " + std::to_string(group));
+        if (plan->impl.kind == SFL_KIND_NS) {
+            sfl::NSPlan& N = *plan->impl.ns;
+            int g = std::min<int>(group, N.S);
+            on_device(plan, [&] {
+                cudaDeviceSynchronize();
+                N.work.alloc(sizeof(float2) * N.H * g);
+            });
+            N.group = g;
+        }
+        return SFL_OK;
+    });
+}
+
+int sfl_analyze(sfl_plan* plan, const void* x, void* c, void* stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(x, "x");
+        need(c, "c");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(c, plan->impl.dtype, "c");
+        on_device(plan, [&] {
+            if (plan->impl.kind == SFL_KIND_NS)
+                sfl::ns_analyze(*plan->impl.ns, x, c, as_stream(stream), false);
+            else
+                sfl::dec_analyze(*plan->impl.dec, x, c, as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
+int sfl_synthesize(sfl_plan* plan, const void* c, void* x, void* stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(x, "x");
+        need(c, "c");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(c, plan->impl.dtype, "c");
+        on_device(plan, [&] {
+            if (plan->impl.kind == SFL_KIND_NS)
+                sfl::ns_synthesize(*plan->impl.ns, c, x, as_stream(stream), false);
+            else
+                sfl::dec_synthesize(*plan->impl.dec, c, x, as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
+int sfl_adjoint_analyze(sfl_plan* plan, const void* c, void* x, void* stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(x, "x");
+        need(c, "c");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(c, plan->impl.dtype, "c");
+        on_device(plan, [&] {
+            if (plan->impl.kind == SFL_KIND_NS)
+                sfl::ns_synthesize(*plan->impl.ns, c, x, as_stream(stream), true);
+            else
+                sfl::dec_adjoint_analyze(*plan->impl.dec, c, x, as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
+int sfl_adjoint_synthesize(sfl_plan* plan, const void* x, void* c, void* stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(x, "x");
+        need(c, "c");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(c, plan->impl.dtype, "c");
+        on_device(plan, [&] {
+            if (plan->impl.kind == SFL_KIND_NS)
+                sfl::ns_analyze(*plan->impl.ns, x, c, as_stream(stream), true);
+            else
+                sfl::dec_adjoint_synthesize(*plan->impl.dec, x, c, as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
+static sfl::NSPlan& ns_of(sfl_plan* plan) {
+    need(plan, "plan");
+    if (plan->impl.kind != SFL_KIND_NS) throw sfl::ArgError("streaming is supported by NSSurfacelet plans only");
+    return *plan->impl.ns;
+}
+
+int sfl_stream_analyze_begin(sfl_plan* plan, const void* x, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(x, "x");
+        on_device(plan, [&] { sfl::ns_stream_analyze_begin(N, x, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
+int sfl_stream_analyze_next(sfl_plan* plan, void* band, int32_t* index, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(band, "band");
+        need(index, "index");
+        int r = SFL_OK, idx = 0;
+        on_device(plan, [&] { r = sfl::ns_stream_analyze_next(N, band, &idx, as_stream(stream)); });
+        if (r == SFL_OK) *index = idx;
+        return r;
+    });
+}
+
+int sfl_stream_synthesize_begin(sfl_plan* plan, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        sfl::ns_stream_synth_begin(N, as_stream(stream));
+        return SFL_OK;
+    });
+}
+
+int sfl_stream_synthesize_next_index(sfl_plan* plan, int32_t* index) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(index, "index");
+        int idx = 0;
+        int r = sfl::ns_stream_synth_next_index(N, &idx);
+        if (r == SFL_OK) *index = idx;
+        return r;
+    });
+}
+
+int sfl_stream_synthesize_push(sfl_plan* plan, const void* band, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(band, "band");
+        on_device(plan, [&] { sfl::ns_stream_synth_push(N, band, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
+int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(x, "x");
+        on_device(plan, [&] { sfl::ns_stream_synth_end(N, x, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const char* name, int32_t index,
+                        double* out, int64_t* count) {
+    return guarded([&] {
+        need(p, "params");
+        need(name, "name");
+        need(count, "count");
+        int d[3];
+        dims_of(dims, d);
+        sfl::NSDesign D = sfl::ns_design(*p, d);
+        const std::vector<double>* v = nullptr;
+        std::string nm(name);
+        if (nm == "m1") {
+            v = &D.m1;
+        } else if (nm == "m2") {
+            v = &D.m2;
+        } else if (nm == "wedge") {
+            int w = index % 64, plane = (index / 64) % 2, hi = (index / 128) % 3, j = index / 384;
+            if (j >= p->scales) throw sfl::ArgError("wedge table index out of range");
+            const sfl::WedgePlanes& W = D.wedges[j][hi][plane];
+            if (w >= (int)W.w.size()) throw sfl::ArgError("wedge table index out of range");
+            v = &W.w[w];
+        } else if (nm == "pa" || nm == "pl") {
+            int lv = index / 3, ax = index % 3;
+            auto& tab = nm == "pa" ? D.pa : D.pl;
+            if (lv < 0 || lv >= (int)tab.size()) throw sfl::ArgError("level out of range");
+            v = &tab[lv][ax];
+        } else {
+            throw sfl::ArgError("unknown table " + nm);
+        }
+        *count = (int64_t)v->size();
+        if (out) std::memcpy(out, v->data(), sizeof(double) * v->size());
+        return SFL_OK;
+    });
+}
+
+int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name, int32_t index,
+                          double* out, int64_t* count) {
+    return guarded([&] {
+        need(p, "params");
+        need(name, "name");
+        need(count, "count");
+        int d[3];
+        dims_of(dims, d);
+        sfl::SurfDesign S = sfl::surf_design(*p, d);
+        std::string nm(name);
+        std::vector<double> tmp;
+        if (nm == "ritf") {
+            int lv = index / 3, K = index % 3;
+            if (lv >= (int)S.scales.size()) throw sfl::ArgError("level out of range");
+            tmp = S.scales[lv].V[K];
+        } else if (nm == "irc") {
+            int which = index % 4, stage = (index / 4) % 32, K = (index / 128) % 3, lv = index / 384;
+            if (lv >= (int)S.scales.size() || stage >= (int)S.scales[lv].stages[K].size())
+                throw sfl::ArgError("stage out of range");
+            const sfl::IRCStage& st = S.scales[lv].stages[K][stage];
+            const std::vector<std::complex<double>>& f = which < 2 ? st.ana[which] : st.syn[which - 2];
+            for (auto z : f) {
+                tmp.push_back(z.real());
+                tmp.push_back(z.imag());
+            }
+        } else if (nm == "pyr_prof") {
+            int lv = index / 3, ax = index % 3;
+            if (lv >= (int)S.pyramid.size()) throw sfl::ArgError("level out of range");
+            tmp = S.pyramid[lv].prof[ax];
+        } else {
+            throw sfl::ArgError("unknown table " + nm);
+        }
+        *count = (int64_t)tmp.size();
+        if (out) std::memcpy(out, tmp.data(), sizeof(double) * tmp.size());
+        return SFL_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,598 @@
+// The decimated Surfacelet on the device: SurfBox's construction as in
+// src/transforms/surfacelet.jl, src/directional/surfacelet_scale.jl,
+// src/directional/irc.jl and src/pyramid/fourier_pyramid.jl.
+//
+// Forward, per channel:
+//   X = FFT(x) (full complex grid; the first pass transforms two real lines
+//   per complex FFT and unpacks both full spectra), then per pyramid level:
+//   split (lowpass cropped to the next level, highpass in place), and per
+//   hourglass K: S_K = X[half_K] V_K / |subband| ; the IRC stages (a 2x2
+//   complex butterfly per bin pair) ; the block inverse FFTs along the two
+//   decimated axes (segmented line passes) ; the C2R along K, two lines per
+//   complex FFT, written straight into the subband's place in the coefficient
+//   vector.  The coarse lowpass is Re(bfft(C))/|C|.
+// Inverse: the mirror image, with one kernel that forms the Hermitian sum of
+// the three hourglasses over the full grid.
+#include <cmath>
+#include <cstring>
+
+#include "passes.cuh"
+#include "plan.h"
+
+namespace sfl {
+
+struct DecStageDev {
+    int m = 0, b = 0;
+    DevMem f[4];   // analysis ch0, ch1, synthesis ch0, ch1: (K-half, m) planes
+};
+
+struct DecLevelDev {
+    int n[3], nlow[3];
+    int cnt[3];
+    DevMem idx[3], idx_low[3], prof[3];
+    float invD15 = 1, D15 = 1;
+    DevMem V[3];
+    int hd[3][3];                     // [K][d] half-K dims
+    std::vector<DecStageDev> stages[3];
+    int counts[3][3];                 // [K][d] block counts
+    int bsize[3][3];                  // [K][d] block size (K: half length)
+    long long first_off[3];           // element offset of hourglass K's first subband
+    long long blk_elems[3];
+    int nsub[3];
+};
+
+struct DecPlan {
+    SurfDesign design;
+    int dims[3];
+    int nch = 1;
+    int J = 0;
+    long long ncoef = 0;
+    std::vector<std::unique_ptr<DecLevelDev>> lv;
+    std::vector<std::unique_ptr<DevMem>> spectra;   // J + 1 full complex grids
+    DevMem S[3];                                   // half-K spectra of level 0 size
+    std::map<int, std::unique_ptr<FFTLen>> ffts;
+};
+
+void DecPlanDeleter::operator()(DecPlan* d) const { delete d; }
+const SurfDesign& dec_design(const DecPlan& d) { return d.design; }
+int dec_nsubbands(const DecPlan& d) { return (int)d.design.sizes.size(); }
+long long dec_ncoeffs(const DecPlan& d) { return d.ncoef; }
+void dec_subband_info(const DecPlan& d, int i, int shape[3], long long* offset) {
+    for (int k = 0; k < 3; ++k) shape[k] = d.design.sizes[i - 1][k];
+    *offset = d.design.offsets[i - 1];
+}
+
+// ── kernels ──────────────────────────────────────────────────────────────────
+
+__device__ __forceinline__ long long lin3(int a, int b, int c, int d0, int d1) {
+    return a + (long long)d0 * (b + (long long)d1 * c);
+}
+
+// src/pyramid/fourier_pyramid.jl:221-231 (file numbering): low = crop(L X)/D^1.5,
+// X[box] *= sqrt(1 - L^2).  `low` must be zeroed first.
+__global__ void pyr_split_kernel(float2* X, float2* low, int n0, int n1, int l0, int l1, const int* i0,
+                                 const int* i1, const int* i2, const int* j0, const int* j1, const int* j2,
+                                 const float* p0, const float* p1, const float* p2, int c0, int c1, int c2,
+                                 float invD15) {
+    long long total = (long long)c0 * c1 * c2;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int a = q % c0;
+        long long r = q / c0;
+        int b = r % c1;
+        int c = r / c1;
+        float L = p0[a] * p1[b] * p2[c];
+        long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
+        float2 v = X[xa];
+        low[lin3(j0[a], j1[b], j2[c], l0, l1)] = c_scale(v, L * invD15);
+        X[xa] = c_scale(v, sqrtf(1.f - L * L));
+    }
+}
+
+// src/pyramid/fourier_pyramid.jl:235-240: X[box] = sqrt(1-L^2) X[box] + L D^1.5 low.
+__global__ void pyr_merge_kernel(float2* X, const float2* low, int n0, int n1, int l0, int l1, const int* i0,
+                                 const int* i1, const int* i2, const int* j0, const int* j1, const int* j2,
+                                 const float* p0, const float* p1, const float* p2, int c0, int c1, int c2,
+                                 float D15) {
+    long long total = (long long)c0 * c1 * c2;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int a = q % c0;
+        long long r = q / c0;
+        int b = r % c1;
+        int c = r / c1;
+        float L = p0[a] * p1[b] * p2[c];
+        long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
+        float2 h = c_scale(X[xa], sqrtf(1.f - L * L));
+        float2 w = c_scale(low[lin3(j0[a], j1[b], j2[c], l0, l1)], L * D15);
+        X[xa] = c_add(h, w);
+    }
+}
+
+// S_K = X[half_K] * V_K * s: src/directional/surfacelet_scale.jl:205-206, 292
+__global__ void hg_mask_kernel(const float2* X, int n0, int n1, float2* S, int h0, int h1, int h2,
+                               const float* V, float s) {
+    long long total = (long long)h0 * h1 * h2;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int a = q % h0;
+        long long r = q / h0;
+        int b = r % h1;
+        int c = r / h1;
+        S[q] = c_scale(X[lin3(a, b, c, n0, n1)], V[q] * s);
+    }
+}
+
+// One IRC stage in place on S (half-K dims h): for every bin pair (A, B) of
+// the 2b-bin groups along axis m, analysis A <- F0(A)A + F0(B)B,
+// B <- F1(A)A + F1(B)B; synthesis A <- G0(A)A + G1(A)B, B <- G0(B)A + G1(B)B.
+// src/directional/irc.jl:304-345 (file numbering)
+__global__ void irc_stage_kernel(float2* S, int h0, int h1, int h2, int K, int m, int b, const float2* f0,
+                                 const float2* f1, int synth) {
+    int hd[3] = {h0, h1, h2};
+    int pd[3] = {h0, h1, h2};
+    pd[m] = hd[m] / 2;
+    long long total = (long long)pd[0] * pd[1] * pd[2];
+    const int nKh = hd[K];
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int c[3];
+        c[0] = q % pd[0];
+        long long r = q / pd[0];
+        c[1] = r % pd[1];
+        c[2] = r / pd[1];
+        int pq = c[m];
+        int cA = (pq / b) * 2 * b + (pq % b);
+        int cB = cA + b;
+        c[m] = cA;
+        long long aA = lin3(c[0], c[1], c[2], h0, h1);
+        c[m] = cB;
+        long long aB = lin3(c[0], c[1], c[2], h0, h1);
+        int kK = c[K];
+        long long fA = kK + (long long)nKh * cA, fB = kK + (long long)nKh * cB;
+        float2 A = S[aA], Bv = S[aB];
+        float2 nA, nB;
+        if (!synth) {
+            nA = c_add(c_mul(f0[fA], A), c_mul(f0[fB], Bv));
+            nB = c_add(c_mul(f1[fA], A), c_mul(f1[fB], Bv));
+        } else {
+            nA = c_add(c_mul(f0[fA], A), c_mul(f1[fA], Bv));
+            nB = c_add(c_mul(f0[fB], A), c_mul(f1[fB], Bv));
+        }
+        S[aA] = nA;
+        S[aB] = nB;
+    }
+}
+
+// X = sum_K (1/3) V_K S_K on each half and the conjugate mirror on the rest:
+// src/directional/surfacelet_scale.jl:231-257
+struct HermArgs {
+    const float2* S[3];
+    const float* V[3];
+};
+__global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs ha, float third) {
+    long long total = (long long)n0 * n1 * n2;
+    int n[3] = {n0, n1, n2};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int k[3];
+        k[0] = q % n0;
+        long long r = q / n0;
+        k[1] = r % n1;
+        k[2] = r / n1;
+        float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int K = 0; K < 3; ++K) {
+            int hd[3] = {n0, n1, n2};
+            hd[K] = n[K] / 2 + 1;
+            if (k[K] < hd[K]) {
+                long long a = lin3(k[0], k[1], k[2], hd[0], hd[1]);
+                v = c_add(v, c_scale(ha.S[K][a], third * ha.V[K][a]));
+            } else {
+                int m0 = (n0 - k[0]) % n0, m1 = (n1 - k[1]) % n1, m2 = (n2 - k[2]) % n2;
+                long long a = lin3(m0, m1, m2, hd[0], hd[1]);
+                v = c_add(v, c_scale(c_conj(ha.S[K][a]), third * ha.V[K][a]));
+            }
+        }
+        X[q] = v;
+    }
+}
+
+// Block <-> subband address map of hourglass K at one level.  Line l of S_K
+// along K is (c_a, c_b) over the two other axes a < b.
+struct BlockMap {
+    int K, ax, bx;
+    int ha;            // extent of S_K along a (lines: l = c_a + ha * c_b)
+    int ba, bb, ca;    // block sizes along a, b; block count along a
+    long long first, blk;
+    int sd0, sd1;      // subband dims along axes 0, 1
+    __device__ __forceinline__ long long addr(int l, int i) const {
+        int c_a = l % ha, c_b = l / ha;
+        int pa = c_a / ba, ra = c_a - pa * ba;
+        int pb = c_b / bb, rb = c_b - pb * bb;
+        int e[3];
+        e[K] = i;
+        e[ax] = ra;
+        e[bx] = rb;
+        return first + (long long)(pa + ca * pb) * blk + e[0] + (long long)sd0 * (e[1] + (long long)sd1 * e[2]);
+    }
+};
+
+// C2R output of two block lines into the subbands (element stride es).
+struct StoreRPairBlocks {
+    float* dst;
+    BlockMap bm;
+    int nlines;
+    int es;
+    __device__ __forceinline__ void operator()(const float2* tile, int npad, int n, int l0, int T, int) const {
+        const int total = T * n;
+        const bool ifast = bm.K == 0;
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            int t, i;
+            if (ifast) {
+                i = idx % n;
+                t = idx / n;
+            } else {
+                t = idx % T;
+                i = idx / T;
+            }
+            int la = 2 * (l0 + t);
+            float2 v = tile[t * npad + i];
+            if (la < nlines) dst[bm.addr(la, i) * es] = v.x;
+            if (la + 1 < nlines) dst[bm.addr(la + 1, i) * es] = v.y;
+        }
+    }
+};
+
+// Two subband lines along K packed as one complex line (R2C input).
+struct LoadRPairBlocks {
+    const float* src;
+    BlockMap bm;
+    int nlines;
+    int es;
+    __device__ __forceinline__ void operator()(float2* tile, int npad, int n, int l0, int T, int) const {
+        const int total = T * n;
+        const bool ifast = bm.K == 0;
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            int t, i;
+            if (ifast) {
+                i = idx % n;
+                t = idx / n;
+            } else {
+                t = idx % T;
+                i = idx / T;
+            }
+            int la = 2 * (l0 + t);
+            float a = la < nlines ? src[bm.addr(la, i) * es] : 0.f;
+            float b = la + 1 < nlines ? src[bm.addr(la + 1, i) * es] : 0.f;
+            tile[t * npad + i] = make_float2(a, b);
+        }
+    }
+};
+
+// ── set-up ───────────────────────────────────────────────────────────────────
+
+template <class T>
+static void upload_vec(DevMem& m, const std::vector<T>& v) {
+    m.alloc(sizeof(T) * (v.empty() ? 1 : v.size()));
+    if (!v.empty()) cuda_check(cudaMemcpy(m.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+}
+
+void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], int dtype) {
+    for (int d = 0; d < 3; ++d)
+        if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
+    std::unique_ptr<DecPlan> D(new DecPlan);
+    D->design = surf_design(p, dims);
+    const SurfDesign& S = D->design;
+    for (int d = 0; d < 3; ++d) D->dims[d] = dims[d];
+    D->nch = dtype == SFL_COMPLEX64 ? 2 : 1;
+    D->J = p.scales;
+    D->ncoef = S.offsets.back();
+    for (int j = 0; j < D->J; ++j) {
+        std::unique_ptr<DecLevelDev> L(new DecLevelDev);
+        const PyrLevel& pl = S.pyramid[j];
+        const ScaleDesign& sc = S.scales[j];
+        for (int d = 0; d < 3; ++d) {
+            L->n[d] = pl.n[d];
+            L->nlow[d] = pl.nlow[d];
+            L->cnt[d] = (int)pl.idx[d].size();
+            upload_vec(L->idx[d], pl.idx[d]);
+            upload_vec(L->idx_low[d], pl.idx_low[d]);
+            std::vector<float> pf(pl.prof[d].begin(), pl.prof[d].end());
+            upload_vec(L->prof[d], pf);
+        }
+        double Dv = (double)pl.D.p / (double)pl.D.q;
+        L->D15 = (float)std::pow(Dv, 1.5);
+        L->invD15 = (float)(1.0 / (double)(float)std::pow(Dv, 1.5));
+        int first = S.level_first[j];   // 0-based index of the level's first subband
+        for (int K = 0; K < 3; ++K) {
+            for (int d = 0; d < 3; ++d) L->hd[K][d] = d == K ? sc.n[K] / 2 + 1 : sc.n[d];
+            std::vector<float> vf(sc.V[K].begin(), sc.V[K].end());
+            upload_vec(L->V[K], vf);
+            for (const IRCStage& st : sc.stages[K]) {
+                DecStageDev sd;
+                sd.m = st.m - 1;
+                sd.b = st.b;
+                const std::vector<std::complex<double>>* src[4] = {&st.ana[0], &st.ana[1], &st.syn[0], &st.syn[1]};
+                for (int w = 0; w < 4; ++w) {
+                    std::vector<float2> f(src[w]->size());
+                    for (size_t i = 0; i < f.size(); ++i)
+                        f[i] = make_float2((float)(*src[w])[i].real(), (float)(*src[w])[i].imag());
+                    upload_vec(sd.f[w], f);
+                }
+                L->stages[K].push_back(std::move(sd));
+            }
+            int nb = 1;
+            for (int d = 0; d < 3; ++d) {
+                L->counts[K][d] = 1 << sc.lv[K][d];
+                L->bsize[K][d] = d == K ? sc.n[K] / 2 + 1 : sc.n[d] / L->counts[K][d];
+                nb *= L->counts[K][d];
+            }
+            L->nsub[K] = nb;
+            L->first_off[K] = S.offsets[first];
+            L->blk_elems[K] = (long long)sc.n[K] * L->bsize[K][(K + 1) % 3] * L->bsize[K][(K + 2) % 3];
+            first += nb;
+        }
+        D->lv.push_back(std::move(L));
+    }
+    // spectra: the input of every level and the coarse lowpass
+    for (int j = 0; j <= D->J; ++j) {
+        const int* n = j < D->J ? S.pyramid[j].n : S.pyramid[D->J - 1].nlow;
+        std::unique_ptr<DevMem> m(new DevMem);
+        m->alloc(sizeof(float2) * (size_t)n[0] * n[1] * n[2]);
+        D->spectra.push_back(std::move(m));
+    }
+    for (int K = 0; K < 3; ++K) {
+        const int* h = D->lv[0]->hd[K];
+        D->S[K].alloc(sizeof(float2) * (size_t)h[0] * h[1] * h[2]);
+    }
+    plan.dec.reset(D.release());
+}
+
+// ── drivers ──────────────────────────────────────────────────────────────────
+
+namespace {
+
+unsigned grid_for(long long total) {
+    long long g = (total + 255) / 256;
+    if (g > 148 * 32) g = 148 * 32;
+    if (g < 1) g = 1;
+    return (unsigned)g;
+}
+
+// Full complex FFT of a real volume (dims d, element stride es) into X.
+void fft_real_full(DecPlan& D, const float* x, int es, const int d[3], float2* X, cudaStream_t st) {
+    Lines gin = axis_lines(d, 0);
+    FFTLen* f0 = get_fft(D.ffts, d[0]);
+    LoadRPair ld{x, ZMap{}, gin, es};
+    StoreFullPair sto{X, ZMap{}, gin};
+    launch_pass(ld, sto, f0->sh, (gin.nlines + 1) / 2, 1, false, st, "dec_fft_r2c");
+    for (int a = 1; a < 3; ++a) {
+        Lines g = axis_lines(d, a);
+        FFTLen* f = get_fft(D.ffts, d[a]);
+        LoadC l2{X, ZMap{}, g, 1.f};
+        StoreC s2{X, ZMap{}, g, 1.f};
+        launch_pass(l2, s2, f->sh, g.nlines, 1, false, st, "dec_fft_c2c");
+    }
+}
+
+// Re(bfft(X)) * scale into a real volume (element stride es).
+void ifft_full_real(DecPlan& D, float2* X, const int d[3], float* out, int es, float scale, cudaStream_t st) {
+    for (int a = 2; a >= 1; --a) {
+        Lines g = axis_lines(d, a);
+        FFTLen* f = get_fft(D.ffts, d[a]);
+        LoadC l2{X, ZMap{}, g, 1.f};
+        StoreC s2{X, ZMap{}, g, 1.f};
+        launch_pass(l2, s2, f->sh, g.nlines, 1, true, st, "dec_fft_c2c");
+    }
+    Lines g0 = axis_lines(d, 0);
+    FFTLen* f0 = get_fft(D.ffts, d[0]);
+    LoadC l0{X, ZMap{}, g0, 1.f};
+    StoreReal s0{out, ZMap{}, g0, es, scale};
+    launch_pass(l0, s0, f0->sh, g0.nlines, 1, true, st, "dec_fft_real");
+}
+
+// Segmented FFTs along axis m of a half-K spectrum: blocks of length bl.
+void block_fft(DecPlan& D, float2* S, const int hd[3], int m, int bl, bool inv, cudaStream_t st) {
+    long long str[3] = {1, hd[0], (long long)hd[0] * hd[1]};
+    int o[2], k = 0;
+    for (int d = 0; d < 3; ++d)
+        if (d != m) o[k++] = d;
+    Lines g;
+    g.B0 = hd[o[0]];
+    g.B1 = hd[o[1]];
+    g.s0 = str[o[0]];
+    g.s1 = str[o[1]];
+    g.s2 = (long long)bl * str[m];
+    g.si = str[m];
+    g.nlines = hd[o[0]] * hd[o[1]] * (hd[m] / bl);
+    FFTLen* f = get_fft(D.ffts, bl);
+    LoadC ld{S, ZMap{}, g, 1.f};
+    StoreC sto{S, ZMap{}, g, 1.f};
+    launch_pass(ld, sto, f->sh, g.nlines, 1, inv, st, "dec_block_fft");
+}
+
+BlockMap block_map(const DecLevelDev& L, int K) {
+    BlockMap bm;
+    bm.K = K;
+    bm.ax = K == 0 ? 1 : 0;
+    bm.bx = K == 2 ? 1 : 2;
+    bm.ha = L.hd[K][bm.ax];
+    bm.ba = L.bsize[K][bm.ax];
+    bm.bb = L.bsize[K][bm.bx];
+    bm.ca = L.counts[K][bm.ax];
+    bm.first = L.first_off[K];
+    bm.blk = L.blk_elems[K];
+    int sd[3];
+    for (int d = 0; d < 3; ++d) sd[d] = d == K ? L.n[K] : L.bsize[K][d];
+    bm.sd0 = sd[0];
+    bm.sd1 = sd[1];
+    return bm;
+}
+
+Lines k_lines(const DecLevelDev& L, int K) {
+    const int* hd = L.hd[K];
+    long long str[3] = {1, hd[0], (long long)hd[0] * hd[1]};
+    int a = K == 0 ? 1 : 0, b = K == 2 ? 1 : 2;
+    Lines g;
+    g.nlines = hd[a] * hd[b];
+    g.B0 = hd[a];
+    g.B1 = hd[b];
+    g.s0 = str[a];
+    g.s1 = str[b];
+    g.s2 = 0;
+    g.si = str[K];
+    return g;
+}
+
+void pyr_split(DecPlan& D, int j, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    float2* X = D.spectra[j]->as<float2>();
+    float2* low = D.spectra[j + 1]->as<float2>();
+    cuda_check(cudaMemsetAsync(low, 0, D.spectra[j + 1]->bytes, st), "memset");
+    long long tot = (long long)L.cnt[0] * L.cnt[1] * L.cnt[2];
+    {
+        int tok = prof_begin("dec_pyr_split", st);
+        pyr_split_kernel<<<grid_for(tot), 256, 0, st>>>(
+            X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
+            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.prof[0].as<float>(),
+            L.prof[1].as<float>(), L.prof[2].as<float>(), L.cnt[0], L.cnt[1], L.cnt[2], L.invD15);
+        prof_end(tok, st);
+    }
+    cuda_check(cudaGetLastError(), "pyr_split_kernel");
+}
+
+void pyr_merge(DecPlan& D, int j, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    float2* X = D.spectra[j]->as<float2>();
+    const float2* low = D.spectra[j + 1]->as<float2>();
+    long long tot = (long long)L.cnt[0] * L.cnt[1] * L.cnt[2];
+    {
+        int tok = prof_begin("dec_pyr_merge", st);
+        pyr_merge_kernel<<<grid_for(tot), 256, 0, st>>>(
+            X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
+            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.prof[0].as<float>(),
+            L.prof[1].as<float>(), L.prof[2].as<float>(), L.cnt[0], L.cnt[1], L.cnt[2], L.D15);
+        prof_end(tok, st);
+    }
+    cuda_check(cudaGetLastError(), "pyr_merge_kernel");
+}
+
+void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    const float2* X = D.spectra[j]->as<float2>();
+    for (int K = 0; K < 3; ++K) {
+        const int* hd = L.hd[K];
+        float2* S = D.S[K].as<float2>();
+        int sb[3];
+        for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
+        float s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
+        long long tot = (long long)hd[0] * hd[1] * hd[2];
+        {
+            int tok = prof_begin("dec_hg_mask", st);
+            hg_mask_kernel<<<grid_for(tot), 256, 0, st>>>(X, L.n[0], L.n[1], S, hd[0], hd[1], hd[2], L.V[K].as<float>(), s);
+            prof_end(tok, st);
+        }
+        cuda_check(cudaGetLastError(), "hg_mask_kernel");
+        for (auto& sg : L.stages[K]) {
+            long long pairs = tot / 2;
+            {
+                int tok = prof_begin("dec_irc", st);
+                irc_stage_kernel<<<grid_for(pairs), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                                                                  sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0);
+                prof_end(tok, st);
+            }
+            cuda_check(cudaGetLastError(), "irc_stage_kernel");
+        }
+        for (int m = 0; m < 3; ++m)
+            if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], true, st);
+        Lines gk = k_lines(L, K);
+        FFTLen* f = get_fft(D.ffts, L.n[K]);
+        LoadHPair ld{S, ZMap{}, gk};
+        StoreRPairBlocks sto{c, block_map(L, K), gk.nlines, es};
+        launch_pass(ld, sto, f->sh, (gk.nlines + 1) / 2, 1, true, st, "dec_c2r_blocks");
+    }
+}
+
+void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    HermArgs ha;
+    for (int K = 0; K < 3; ++K) {
+        const int* hd = L.hd[K];
+        float2* S = D.S[K].as<float2>();
+        Lines gk = k_lines(L, K);
+        FFTLen* f = get_fft(D.ffts, L.n[K]);
+        LoadRPairBlocks ld{c, block_map(L, K), gk.nlines, es};
+        StoreHalfPair sto{S, ZMap{}, gk};
+        launch_pass(ld, sto, f->sh, (gk.nlines + 1) / 2, 1, false, st, "dec_r2c_blocks");
+        for (int m = 0; m < 3; ++m)
+            if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
+        long long tot = (long long)hd[0] * hd[1] * hd[2];
+        for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
+            auto& sg = L.stages[K][s];
+            {
+                int tok = prof_begin("dec_irc", st);
+                irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                                                                    sg.f[2].as<float2>(), sg.f[3].as<float2>(), 1);
+                prof_end(tok, st);
+            }
+            cuda_check(cudaGetLastError(), "irc_stage_kernel");
+        }
+        ha.S[K] = S;
+        ha.V[K] = L.V[K].as<float>();
+    }
+    long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
+    {
+        int tok = prof_begin("dec_herm_sum", st);
+        hermitian_sum_kernel<<<grid_for(tot), 256, 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
+                                                             1.0f / 3.0f);
+        prof_end(tok, st);
+    }
+    cuda_check(cudaGetLastError(), "hermitian_sum_kernel");
+}
+
+}  // namespace
+
+void dec_analyze(DecPlan& D, const void* x, void* c, cudaStream_t st) {
+    const int es = D.nch;
+    const SurfDesign& S = D.design;
+    for (int ch = 0; ch < D.nch; ++ch) {
+        const float* xin = reinterpret_cast<const float*>(x) + ch;
+        float* cout = reinterpret_cast<float*>(c) + ch;
+        fft_real_full(D, xin, es, D.dims, D.spectra[0]->as<float2>(), st);
+        for (int j = 0; j < D.J; ++j) {
+            pyr_split(D, j, st);
+            scale_forward(D, j, cout, es, st);
+        }
+        const int* nl = S.pyramid[D.J - 1].nlow;
+        float scale = (float)(1.0 / ((double)nl[0] * nl[1] * nl[2]));
+        ifft_full_real(D, D.spectra[D.J]->as<float2>(), nl, cout, es, scale, st);
+    }
+}
+
+void dec_synthesize(DecPlan& D, const void* c, void* x, cudaStream_t st) {
+    const int es = D.nch;
+    const SurfDesign& S = D.design;
+    for (int ch = 0; ch < D.nch; ++ch) {
+        const float* cin = reinterpret_cast<const float*>(c) + ch;
+        float* xout = reinterpret_cast<float*>(x) + ch;
+        const int* nl = S.pyramid[D.J - 1].nlow;
+        fft_real_full(D, cin, es, nl, D.spectra[D.J]->as<float2>(), st);
+        for (int j = D.J - 1; j >= 0; --j) {
+            scale_inverse(D, j, cin, es, st);
+            pyr_merge(D, j, st);
+        }
+        float scale = (float)(1.0 / ((double)D.dims[0] * D.dims[1] * D.dims[2]));
+        ifft_full_real(D, D.spectra[0]->as<float2>(), D.dims, xout, es, scale, st);
+    }
+}
+
+void dec_adjoint_analyze(DecPlan&, const void*, void*, cudaStream_t) {
+    throw ArgError("the adjoint of the decimated transform is not available in this build");
+}
+
+void dec_adjoint_synthesize(DecPlan&, const void*, void*, cudaStream_t) {
+    throw ArgError("the adjoint of the decimated transform is not available in this build");
+}
+
+}  // namespace sfl

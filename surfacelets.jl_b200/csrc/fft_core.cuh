@@ -1,0 +1,230 @@
+// Shared-memory mixed-radix Stockham FFT core for sm_100a, and the line
+// geometry the pass kernels use to stage tiles of lines through it.
+//
+// A CTA stages T lines of length n in shared memory (row pitch npad = n + 1
+// so that 64-bit accesses of consecutive lines hit distinct banks), runs the
+// Stockham stages with radix 8, 5, 4, 3, 2 (and a direct DFT for any other
+// prime factor), and hands the tile back to a store op.  Twiddles come from a
+// float64-designed table of e^{-2 pi i t/n}, staged in shared memory.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sfl {
+
+constexpr int kMaxStages = 24;
+
+struct FFTShape {
+    int n = 1;
+    int nstages = 0;
+    int radix[kMaxStages] = {};
+    const float2* tw = nullptr;   // device: n entries, e^{-2 pi i t / n}
+};
+
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse)
+__device__ __forceinline__ float2 c_rot(float2 a, bool inv) {
+    return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <int R>
+struct Dft;
+
+template <>
+struct Dft<2> {
+    __device__ __forceinline__ static void run(float2* v, bool) {
+        float2 a = v[0], b = v[1];
+        v[0] = c_add(a, b);
+        v[1] = c_sub(a, b);
+    }
+};
+
+template <>
+struct Dft<3> {
+    __device__ __forceinline__ static void run(float2* v, bool inv) {
+        const float c = -0.5f;
+        const float s = inv ? -0.86602540378443864676f : 0.86602540378443864676f;
+        float2 t1 = c_add(v[1], v[2]);
+        float2 t2 = c_sub(v[1], v[2]);
+        float2 m = make_float2(v[0].x + c * t1.x, v[0].y + c * t1.y);
+        // -i s t2
+        float2 r = make_float2(s * t2.y, -s * t2.x);
+        v[0] = c_add(v[0], t1);
+        v[1] = c_add(m, r);
+        v[2] = c_sub(m, r);
+    }
+};
+
+template <>
+struct Dft<4> {
+    __device__ __forceinline__ static void run(float2* v, bool inv) {
+        float2 t0 = c_add(v[0], v[2]);
+        float2 t1 = c_sub(v[0], v[2]);
+        float2 t2 = c_add(v[1], v[3]);
+        float2 t3 = c_rot(c_sub(v[1], v[3]), inv);
+        v[0] = c_add(t0, t2);
+        v[2] = c_sub(t0, t2);
+        v[1] = c_add(t1, t3);
+        v[3] = c_sub(t1, t3);
+    }
+};
+
+template <>
+struct Dft<5> {
+    __device__ __forceinline__ static void run(float2* v, bool inv) {
+        const float c1 = 0.30901699437494742410f;    // cos(2pi/5)
+        const float c2 = -0.80901699437494742410f;   // cos(4pi/5)
+        const float s1 = inv ? -0.95105651629515357212f : 0.95105651629515357212f;   // sin(2pi/5)
+        const float s2 = inv ? -0.58778525229247312917f : 0.58778525229247312917f;   // sin(4pi/5)
+        float2 a14 = c_add(v[1], v[4]), d14 = c_sub(v[1], v[4]);
+        float2 a23 = c_add(v[2], v[3]), d23 = c_sub(v[2], v[3]);
+        float2 m1 = make_float2(v[0].x + c1 * a14.x + c2 * a23.x, v[0].y + c1 * a14.y + c2 * a23.y);
+        float2 m2 = make_float2(v[0].x + c2 * a14.x + c1 * a23.x, v[0].y + c2 * a14.y + c1 * a23.y);
+        // r1 = s1 d14 + s2 d23 ; r2 = s2 d14 - s1 d23 ; X1 = m1 - i r1 ; X2 = m2 - i r2
+        float2 r1 = make_float2(s1 * d14.x + s2 * d23.x, s1 * d14.y + s2 * d23.y);
+        float2 r2 = make_float2(s2 * d14.x - s1 * d23.x, s2 * d14.y - s1 * d23.y);
+        v[0] = make_float2(v[0].x + a14.x + a23.x, v[0].y + a14.y + a23.y);
+        v[1] = make_float2(m1.x + r1.y, m1.y - r1.x);
+        v[4] = make_float2(m1.x - r1.y, m1.y + r1.x);
+        v[2] = make_float2(m2.x + r2.y, m2.y - r2.x);
+        v[3] = make_float2(m2.x - r2.y, m2.y + r2.x);
+    }
+};
+
+template <>
+struct Dft<8> {
+    __device__ __forceinline__ static void run(float2* v, bool inv) {
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4>::run(e, inv);
+        Dft<4>::run(o, inv);
+        const float h = 0.70710678118654752440f;
+        // w8^1 = h(1 -+ i), w8^2 = -+i, w8^3 = h(-1 -+ i)
+        float2 o1 = inv ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                        : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+        float2 o2 = c_rot(o[2], inv);
+        float2 o3 = inv ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                        : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+        v[0] = c_add(e[0], o[0]);
+        v[4] = c_sub(e[0], o[0]);
+        v[1] = c_add(e[1], o1);
+        v[5] = c_sub(e[1], o1);
+        v[2] = c_add(e[2], o2);
+        v[6] = c_sub(e[2], o2);
+        v[3] = c_add(e[3], o3);
+        v[7] = c_sub(e[3], o3);
+    }
+};
+
+__device__ __forceinline__ float2 twiddle(const float2* tw, int idx, bool inv) {
+    float2 w = tw[idx];
+    return inv ? make_float2(w.x, -w.y) : w;
+}
+
+// One Stockham stage of radix R over T lines (in -> out).
+template <int R>
+__device__ __forceinline__ void stockham_stage(const float2* __restrict__ in, float2* __restrict__ out, int T,
+                                               int n, int npad, int Ns, const float2* tw, bool inv) {
+    const int nb = n / R;
+    const int total = T * nb;
+    const int tstep = n / (Ns * R);
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        int t = idx / nb;
+        int j = idx - t * nb;
+        const float2* x = in + t * npad;
+        float2* y = out + t * npad;
+        int k = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = x[j + r * nb];
+        if (Ns > 1) {
+            int step = k * tstep;
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = c_mul(v[r], twiddle(tw, r * step, inv));
+        }
+        Dft<R>::run(v, inv);
+        int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) y[base + r * Ns] = v[r];
+    }
+}
+
+// A stage of any radix R (used for prime factors without a dedicated
+// butterfly): each output is a direct sum over the R inputs.
+__device__ __forceinline__ void stockham_stage_generic(const float2* __restrict__ in, float2* __restrict__ out,
+                                                       int R, int T, int n, int npad, int Ns, const float2* tw,
+                                                       bool inv) {
+    const int nb = n / R;
+    const int total = T * nb * R;
+    const int tstep = n / (Ns * R);
+    const int rstep = n / R;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        int m = idx % R;
+        int q = idx / R;
+        int t = q / nb;
+        int j = q - t * nb;
+        const float2* x = in + t * npad;
+        float2* y = out + t * npad;
+        int k = j % Ns;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int r = 0; r < R; ++r) {
+            float2 v = x[j + r * nb];
+            if (Ns > 1 && r > 0) v = c_mul(v, twiddle(tw, r * k * tstep, inv));
+            int e = (r * m) % R;
+            acc = c_add(acc, e ? c_mul(v, twiddle(tw, e * rstep, inv)) : v);
+        }
+        y[(j / Ns) * Ns * R + k + m * Ns] = acc;
+    }
+}
+
+// All stages; returns the buffer that holds the result (a or b).
+__device__ __forceinline__ float2* fft_tile(float2* a, float2* b, int T, const FFTShape& sh, int npad,
+                                            const float2* tw, bool inv) {
+    int Ns = 1;
+    for (int s = 0; s < sh.nstages; ++s) {
+        int R = sh.radix[s];
+        switch (R) {
+            case 2: stockham_stage<2>(a, b, T, sh.n, npad, Ns, tw, inv); break;
+            case 3: stockham_stage<3>(a, b, T, sh.n, npad, Ns, tw, inv); break;
+            case 4: stockham_stage<4>(a, b, T, sh.n, npad, Ns, tw, inv); break;
+            case 5: stockham_stage<5>(a, b, T, sh.n, npad, Ns, tw, inv); break;
+            case 8: stockham_stage<8>(a, b, T, sh.n, npad, Ns, tw, inv); break;
+            default: stockham_stage_generic(a, b, R, T, sh.n, npad, Ns, tw, inv); break;
+        }
+        __syncthreads();
+        float2* t = a;
+        a = b;
+        b = t;
+        Ns *= R;
+    }
+    return a;
+}
+
+// Lines of a strided array: line l -> (l0, l1, l2) with l0 fastest; element i
+// of line l sits at l0*s0 + l1*s1 + l2*s2 + i*si.
+struct Lines {
+    int nlines = 0;
+    int B0 = 1, B1 = 1;
+    long long s0 = 0, s1 = 0, s2 = 0, si = 0;
+    __device__ __forceinline__ long long base(int l) const {
+        int l0 = l % B0;
+        int r = l / B0;
+        int l1 = r % B1;
+        int l2 = r / B1;
+        return (long long)l0 * s0 + (long long)l1 * s1 + (long long)l2 * s2;
+    }
+};
+
+// Shared-memory layout of a pass: [twiddles n][tile a T*npad][tile b T*npad] (+ extra).
+__device__ __forceinline__ void load_twiddles(float2* tws, const FFTShape& sh) {
+    for (int i = threadIdx.x; i < sh.n; i += blockDim.x) tws[i] = sh.tw[i];
+}
+
+}  // namespace sfl

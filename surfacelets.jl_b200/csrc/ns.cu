@@ -1,0 +1,517 @@
+// NSSurfacelet on the device: the cascade of src/transforms/ns_surfacelet.jl
+// as line passes over the rfft grid (h1, n2, n3).
+//
+//   analysis, per subband s:   c_s = irfft(X * M_s)
+//     pass 3 (axis 3, inverse) loads X and multiplies by M_s on the fly,
+//     pass 2 (axis 2, inverse), pass 1 (axis 1, C2R of two lines at once,
+//     scaled by 1/N) writes c_s straight into the coefficient array.
+//   synthesis:                 x = irfft(sum_s rfft(c_s) * M_s)
+//     pass 1 (R2C of two lines at once), pass 2, then pass 3 runs the FFT of
+//     every subband of a group in one CTA and accumulates M_s * F_s in
+//     registers with Kahan compensation; one accumulator round trip per group.
+//
+// M_s = B_j * hg_i * w_a * w_b is evaluated per element from the float32
+// tables (m1 on the grid, m2 and the wedge planes on planes, the pyramid
+// factors on axes), never materialized.
+#include <cmath>
+#include <cstring>
+
+#include "passes.cuh"
+#include "plan.h"
+
+namespace sfl {
+
+// Mask of item `it` at rfft-grid point (k1, k2, k3).  synth selects the
+// synthesis mask, which is B_j alone when the bank is not tight
+// (src/transforms/ns_surfacelet.jl:226-227, 237-238).
+__device__ __forceinline__ float ns_mask(const NSMaskTables& tb, const NSItem& it, int k1, int k2, int k3,
+                                         bool synth) {
+    const float* v = tb.vec;
+    const int L = it.lv;
+    if (it.kind == 1) {
+        // lowpass a1 a2 a3: src/transforms/ns_surfacelet.jl:358-371
+        return v[tb.pa_off[L][0] + k1] * v[tb.pa_off[L][1] + k2] * v[tb.pa_off[L][2] + k3];
+    }
+    // B_j: src/transforms/ns_surfacelet.jl:271-272
+    float a = v[tb.pa_off[L][0] + k1] * v[tb.pa_off[L][1] + k2] * v[tb.pa_off[L][2] + k3];
+    float l = v[tb.pl_off[L][0] + k1] * v[tb.pl_off[L][1] + k2] * v[tb.pl_off[L][2] + k3];
+    float B = a * sqrtf(fmaxf(1.f - l * l, 0.f));
+    if (synth && !tb.tight) return B;
+    // hourglass factor: src/transforms/ns_surfacelet.jl:265-268, hourglass.jl:289-303
+    float f1 = tb.m1[k1 + (long long)tb.h1 * (k2 + (long long)tb.n2 * k3)];
+    float f2 = tb.m2[k2 + (long long)tb.n2 * k3];
+    float w1 = it.i == 1 ? f1 : 1.f - f1;
+    float w2 = it.i == 1 ? 1.f : (it.i == 2 ? f2 : 1.f - f2);
+    float w = w1 * w2;
+    float hg = tb.tight ? sqrtf(fmaxf(w, 0.f)) : w;
+    // wedge planes: src/transforms/ns_surfacelet.jl:376-427
+    int kk[3] = {k1, k2, k3};
+    float wa = tb.planes[it.wa_off + kk[it.wa_lo] + it.wa_dlo * kk[it.wa_hi]];
+    float wb = tb.planes[it.wb_off + kk[it.wb_lo] + it.wb_dlo * kk[it.wb_hi]];
+    return ((B * hg) * wa) * wb;
+}
+
+// Pass-3 load of the analysis: lines along axis 3 of X, times the mask of
+// item z.  Line l = (k1, k2) with k1 fastest.
+struct LoadNSMask {
+    const float2* X;
+    NSMaskTables tb;
+    const NSItem* items;
+    int item0;
+    int synth;
+    __device__ __forceinline__ void operator()(float2* tile, int npad, int n, int l0, int T, int z) const {
+        const NSItem it = items[item0 + z];
+        const int nlines = tb.h1 * tb.n2;
+        const long long si = (long long)tb.h1 * tb.n2;
+        const int total = T * n;
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            int t = idx % T;
+            int i = idx / T;
+            int l = l0 + t;
+            float2 v = make_float2(0.f, 0.f);
+            if (l < nlines) {
+                int k1 = l % tb.h1, k2 = l / tb.h1;
+                v = c_scale(X[l + (long long)i * si], ns_mask(tb, it, k1, k2, i, synth != 0));
+            }
+            tile[t * npad + i] = v;
+        }
+    }
+};
+
+constexpr int kAccMax = 16;   // accumulator registers per thread (tile elements / 256)
+
+// Pass 3 of the synthesis: for every item of the group, load its lines along
+// axis 3 from work + z*H, FFT, multiply by its mask and accumulate, with Kahan
+// compensation, into registers; then one round trip of acc/comp.
+__global__ void __launch_bounds__(256) ns_accum_kernel(const float2* __restrict__ work, long long H, int G,
+                                                       NSMaskTables tb, const NSItem* __restrict__ items,
+                                                       int item0, int synth, float2* acc, float2* comp, int init,
+                                                       FFTShape sh, int T, int npad) {
+    extern __shared__ float2 smem[];
+    float2* tw = smem;
+    float2* a = smem + sh.n + (sh.n & 1);
+    float2* b = a + T * npad;
+    load_twiddles(tw, sh);
+    const int n = sh.n;
+    const int nlines = tb.h1 * tb.n2;
+    const long long si = (long long)tb.h1 * tb.n2;
+    const int l0 = blockIdx.x * T;
+    const int total = T * n;
+    float2 s[kAccMax], c[kAccMax];
+#pragma unroll
+    for (int e = 0; e < kAccMax; ++e) {
+        s[e] = make_float2(0.f, 0.f);
+        c[e] = make_float2(0.f, 0.f);
+    }
+    if (!init) {
+#pragma unroll
+        for (int e = 0; e < kAccMax; ++e) {
+            int idx = threadIdx.x + e * blockDim.x;
+            if (idx < total) {
+                int t = idx % T, i = idx / T, l = l0 + t;
+                if (l < nlines) {
+                    s[e] = acc[l + (long long)i * si];
+                    c[e] = comp[l + (long long)i * si];
+                }
+            }
+        }
+    }
+    for (int z = 0; z < G; ++z) {
+        const float2* src = work + (long long)z * H;
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+            int t = idx % T, i = idx / T, l = l0 + t;
+            a[t * npad + i] = l < nlines ? src[l + (long long)i * si] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        float2* r = fft_tile(a, b, T, sh, npad, tw, false);
+        const NSItem it = items[item0 + z];
+#pragma unroll
+        for (int e = 0; e < kAccMax; ++e) {
+            int idx = threadIdx.x + e * blockDim.x;
+            if (idx < total) {
+                int t = idx % T, i = idx / T, l = l0 + t;
+                if (l < nlines) {
+                    int k1 = l % tb.h1, k2 = l / tb.h1;
+                    float m = ns_mask(tb, it, k1, k2, i, synth != 0);
+                    float2 v = c_scale(r[t * npad + i], m);
+                    // Kahan: y = v - c ; t = s + y ; c = (t - s) - y ; s = t
+                    float2 y = c_sub(v, c[e]);
+                    float2 tt = c_add(s[e], y);
+                    c[e] = c_sub(c_sub(tt, s[e]), y);
+                    s[e] = tt;
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int e = 0; e < kAccMax; ++e) {
+        int idx = threadIdx.x + e * blockDim.x;
+        if (idx < total) {
+            int t = idx % T, i = idx / T, l = l0 + t;
+            if (l < nlines) {
+                acc[l + (long long)i * si] = s[e];
+                comp[l + (long long)i * si] = c[e];
+            }
+        }
+    }
+}
+
+// ── set-up ───────────────────────────────────────────────────────────────────
+
+static std::vector<int> factorize(int n) {
+    std::vector<int> f;
+    for (int r : {8, 4, 2, 3, 5}) {
+        while (n % r == 0) {
+            f.push_back(r);
+            n /= r;
+        }
+    }
+    for (int p = 7; n > 1; p += 2) {
+        while (n % p == 0) {
+            f.push_back(p);
+            n /= p;
+        }
+    }
+    return f;
+}
+
+FFTLen* get_fft(std::map<int, std::unique_ptr<FFTLen>>& cache, int n) {
+    auto it = cache.find(n);
+    if (it != cache.end()) return it->second.get();
+    std::unique_ptr<FFTLen> f(new FFTLen);
+    std::vector<int> r = factorize(n);
+    if ((int)r.size() > kMaxStages) throw ArgError("FFT length has too many factors");
+    f->sh.n = n;
+    f->sh.nstages = (int)r.size();
+    for (size_t i = 0; i < r.size(); ++i) f->sh.radix[i] = r[i];
+    std::vector<float2> tw(n);
+    for (int t = 0; t < n; ++t) {
+        // e^{-2 pi i t/n} designed in float64
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)t / (long double)n;
+        tw[t] = make_float2((float)std::cos((double)a), (float)std::sin((double)a));
+    }
+    f->tw.alloc(sizeof(float2) * n);
+    cuda_check(cudaMemcpy(f->tw.p, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice), "twiddle upload");
+    f->sh.tw = f->tw.as<float2>();
+    FFTLen* raw = f.get();
+    cache[n] = std::move(f);
+    return raw;
+}
+
+template <class T>
+static void upload(DevMem& m, const std::vector<T>& v) {
+    m.alloc(sizeof(T) * (v.empty() ? 1 : v.size()));
+    if (!v.empty()) cuda_check(cudaMemcpy(m.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+}
+
+static std::vector<float> to_f32(const std::vector<double>& v) {
+    std::vector<float> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
+    return o;
+}
+
+void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype) {
+    for (int d = 0; d < 3; ++d)
+        if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
+    P.design = ns_design(p, dims);
+    const NSDesign& D = P.design;
+    P.p = p;
+    for (int d = 0; d < 3; ++d) P.dims[d] = dims[d];
+    P.h1 = dims[0] / 2 + 1;
+    P.N = (long long)dims[0] * dims[1] * dims[2];
+    P.H = (long long)P.h1 * dims[1] * dims[2];
+    P.S = ns_nsubbands(p);
+    P.nch = dtype == SFL_COMPLEX64 ? 2 : 1;
+    const int J = p.scales;
+
+    // tables
+    upload(P.m1, to_f32(D.m1));
+    upload(P.m2, to_f32(D.m2));
+    std::vector<float> vec;
+    NSMaskTables& tb = P.tb;
+    for (int lv = 0; lv <= J; ++lv)
+        for (int d = 0; d < 3; ++d) {
+            tb.pa_off[lv][d] = (int)vec.size();
+            for (double x : D.pa[lv][d]) vec.push_back((float)x);
+        }
+    for (int lv = 0; lv < J; ++lv)
+        for (int d = 0; d < 3; ++d) {
+            tb.pl_off[lv][d] = (int)vec.size();
+            for (double x : D.pl[lv][d]) vec.push_back((float)x);
+        }
+    upload(P.vec, vec);
+    std::vector<float> planes;
+    // plane_off[j][i][plane][w]
+    std::vector<std::array<std::array<std::vector<int>, 2>, 3>> off(J);
+    for (int j = 0; j < J; ++j)
+        for (int i = 0; i < 3; ++i)
+            for (int q = 0; q < 2; ++q) {
+                const WedgePlanes& W = D.wedges[j][i][q];
+                for (const auto& w : W.w) {
+                    off[j][i][q].push_back((int)planes.size());
+                    for (double x : w) planes.push_back((float)x);
+                }
+            }
+    upload(P.planes, planes);
+    tb.m1 = P.m1.as<float>();
+    tb.m2 = P.m2.as<float>();
+    tb.vec = P.vec.as<float>();
+    tb.planes = P.planes.as<float>();
+    tb.h1 = P.h1;
+    tb.n2 = dims[1];
+    tb.n3 = dims[2];
+    tb.tight = p.tight ? 1 : 0;
+
+    // items in streaming order: directional subbands ascending, then the lowpass.
+    // Subband index: src/transforms/ns_surfacelet.jl:222-242, 430
+    std::vector<NSItem> items;
+    int offset = 1;
+    for (int j = 1; j <= J; ++j) {
+        int L = p.direction_levels[j - 1];
+        int na = 1 << ((L + 1) / 2), nb = 1 << (L / 2);
+        for (int i = 1; i <= 3; ++i)
+            for (int a = 1; a <= na; ++a)
+                for (int b = 1; b <= nb; ++b) {
+                    NSItem it{};
+                    it.s = offset + ((i - 1) * na + (a - 1)) * nb + b;
+                    it.kind = 0;
+                    it.lv = J - j;
+                    it.i = i;
+                    const WedgePlanes& Wa = D.wedges[j - 1][i - 1][0];
+                    const WedgePlanes& Wb = D.wedges[j - 1][i - 1][1];
+                    it.wa_off = off[j - 1][i - 1][0][a - 1];
+                    it.wb_off = off[j - 1][i - 1][1][b - 1];
+                    it.wa_lo = Wa.lo - 1;
+                    it.wa_hi = Wa.hi - 1;
+                    it.wa_dlo = Wa.dlo;
+                    it.wb_lo = Wb.lo - 1;
+                    it.wb_hi = Wb.hi - 1;
+                    it.wb_dlo = Wb.dlo;
+                    items.push_back(it);
+                }
+        offset += 3 * na * nb;
+    }
+    NSItem low{};
+    low.s = 1;
+    low.kind = 1;
+    low.lv = J;
+    low.i = 1;
+    items.push_back(low);
+    P.items_host = items;
+    upload(P.items, items);
+
+    get_fft(P.ffts, dims[0]);
+    get_fft(P.ffts, dims[1]);
+    get_fft(P.ffts, dims[2]);
+
+    P.X.alloc(sizeof(float2) * P.H * P.nch);
+    P.group = std::min(8, P.S);
+    P.work.alloc(sizeof(float2) * P.H * P.group);
+    P.acc.alloc(sizeof(float2) * P.H * P.nch);
+    P.comp.alloc(sizeof(float2) * P.H * P.nch);
+}
+
+// ── passes ───────────────────────────────────────────────────────────────────
+
+namespace {
+
+// rfft grid of the plan
+struct Grid {
+    int d[3];
+};
+
+Grid half_grid(const NSPlan& P) { return Grid{{P.h1, P.dims[1], P.dims[2]}}; }
+
+// R2C along axis 1 of nz real volumes (element stride es) into nz spectra.
+void pass_r2c(NSPlan& P, const float* src, ZMap zin, int es, float2* dst, long long dst_zstride, int nz,
+              cudaStream_t st) {
+    FFTLen* f = get_fft(P.ffts, P.dims[0]);
+    Lines gin = axis_lines(P.dims, 0);
+    Grid hg = half_grid(P);
+    Lines gout = axis_lines(hg.d, 0);
+    LoadRPair ld{src, zin, gin, es};
+    ZMap zo;
+    zo.zstride = dst_zstride;
+    StoreHalfPair sto{dst, zo, gout};
+    launch_pass(ld, sto, f->sh, (gin.nlines + 1) / 2, nz, false, st, "ns_r2c_axis1");
+}
+
+// C2R along axis 1 of nz spectra into nz real volumes, scaled.
+void pass_c2r(NSPlan& P, const float2* src, long long src_zstride, float* dst, ZMap zout, int es, float scale,
+              int nz, cudaStream_t st) {
+    FFTLen* f = get_fft(P.ffts, P.dims[0]);
+    Grid hg = half_grid(P);
+    Lines gin = axis_lines(hg.d, 0);
+    Lines gout = axis_lines(P.dims, 0);
+    ZMap zi;
+    zi.zstride = src_zstride;
+    LoadHPair ld{src, zi, gin};
+    StoreRPair sto{dst, zout, gout, es, scale};
+    launch_pass(ld, sto, f->sh, (gout.nlines + 1) / 2, nz, true, st, "ns_c2r_axis1");
+}
+
+// Complex FFT along axis a (1 or 2, 0-based) of nz spectra.
+void pass_c2c(NSPlan& P, const float2* src, float2* dst, long long zstride, int axis, bool inv, int nz,
+              cudaStream_t st) {
+    Grid hg = half_grid(P);
+    FFTLen* f = get_fft(P.ffts, hg.d[axis]);
+    Lines g = axis_lines(hg.d, axis);
+    ZMap zm;
+    zm.zstride = zstride;
+    LoadC ld{src, zm, g, 1.f};
+    StoreC sto{dst, zm, g, 1.f};
+    launch_pass(ld, sto, f->sh, g.nlines, nz, inv, st, axis == 1 ? "ns_c2c_axis2" : "ns_c2c_axis3");
+}
+
+// The coefficient subbands of items [i0, ...): subband s at (s-1)*N*es.
+ZMap subband_map(NSPlan& P, int i0, int es) {
+    ZMap zc;
+    zc.items = P.items.as<NSItem>();
+    zc.item0 = i0;
+    zc.sub_stride = P.N * es;
+    return zc;
+}
+
+void rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
+    pass_r2c(P, x, ZMap{}, es, X, 0, 1, st);
+    pass_c2c(P, X, X, 0, 1, false, 1, st);
+    pass_c2c(P, X, X, 0, 2, false, 1, st);
+}
+
+void irfft3(NSPlan& P, const float2* A, float* x, int es, cudaStream_t st) {
+    float2* W = P.work.as<float2>();
+    pass_c2c(P, A, W, 0, 2, true, 1, st);
+    pass_c2c(P, W, W, 0, 1, true, 1, st);
+    pass_c2r(P, W, 0, x, ZMap{}, es, 1.0f / (float)P.N, 1, st);
+}
+
+// Analysis of items [i0, i0 + nz) from spectrum X into the coefficients
+// (item z written at cbase + zc.off(z), element stride es).
+void analyze_items(NSPlan& P, const float2* X, float* cbase, ZMap zc, int es, int i0, int nz, bool synth_masks,
+                   cudaStream_t st) {
+    float2* W = P.work.as<float2>();
+    Grid hg = half_grid(P);
+    FFTLen* f3 = get_fft(P.ffts, P.dims[2]);
+    LoadNSMask ld{X, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0};
+    Lines g3 = axis_lines(hg.d, 2);
+    ZMap zw;
+    zw.zstride = P.H;
+    StoreC sto{W, zw, g3, 1.f};
+    launch_pass(ld, sto, f3->sh, g3.nlines, nz, true, st, "ns_mask_axis3");
+    pass_c2c(P, W, W, P.H, 1, true, nz, st);
+    pass_c2r(P, W, P.H, cbase, zc, es, 1.0f / (float)P.N, nz, st);
+}
+
+// Synthesis accumulation of items [i0, i0 + nz) read from the coefficients
+// (item z at cbase + zc.off(z)) into acc/comp.
+void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz, bool analysis_masks, float2* acc,
+                 float2* comp, bool init, cudaStream_t st) {
+    float2* W = P.work.as<float2>();
+    pass_r2c(P, cbase, zc, es, W, P.H, nz, st);
+    pass_c2c(P, W, W, P.H, 1, false, nz, st);
+    FFTLen* f3 = get_fft(P.ffts, P.dims[2]);
+    int n = f3->sh.n;
+    int T = pass_tile(n);
+    while (T > 1 && T * n > kAccMax * 256) --T;
+    if (T * n > kAccMax * 256) throw ArgError("axis 3 is too long for the accumulating pass of this build");
+    int npad = n + 1;
+    size_t smem = pass_smem_bytes(n, T);
+    static bool configured = false;
+    if (!configured) {
+        cuda_check(cudaFuncSetAttribute(ns_accum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    int nlines = P.h1 * P.dims[1];
+    dim3 grid((nlines + T - 1) / T);
+    int tok = prof_begin("ns_accum_axis3", st);
+    ns_accum_kernel<<<grid, 256, smem, st>>>(W, P.H, nz, P.tb, P.items.as<NSItem>(), i0,
+                                             analysis_masks ? 0 : 1, acc, comp, init ? 1 : 0,
+                                             f3->sh, T, npad);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "ns_accum_kernel launch");
+}
+
+}  // namespace
+
+void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
+    const int es = P.nch;
+    for (int ch = 0; ch < P.nch; ++ch) {
+        float2* X = P.X.as<float2>();
+        rfft3(P, reinterpret_cast<const float*>(x) + ch, es, X, st);
+        for (int i0 = 0; i0 < P.S; i0 += P.group) {
+            int nz = std::min(P.group, P.S - i0);
+            analyze_items(P, X, reinterpret_cast<float*>(c) + ch, subband_map(P, i0, es), es, i0, nz, synth_masks,
+                          st);
+        }
+    }
+}
+
+void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
+    const int es = P.nch;
+    for (int ch = 0; ch < P.nch; ++ch) {
+        float2* A = P.acc.as<float2>();
+        for (int i0 = 0; i0 < P.S; i0 += P.group) {
+            int nz = std::min(P.group, P.S - i0);
+            synth_items(P, reinterpret_cast<const float*>(c) + ch, subband_map(P, i0, es), es, i0, nz,
+                        analysis_masks, A, P.comp.as<float2>(), i0 == 0, st);
+        }
+        irfft3(P, A, reinterpret_cast<float*>(x) + ch, es, st);
+    }
+}
+
+// ── streaming ────────────────────────────────────────────────────────────────
+
+void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
+    for (int ch = 0; ch < P.nch; ++ch)
+        rfft3(P, reinterpret_cast<const float*>(x) + ch, P.nch, P.X.as<float2>() + ch * P.H, st);
+    P.stream_mode = 1;
+    P.stream_pos = 0;
+}
+
+int ns_stream_analyze_next(NSPlan& P, void* band, int* index, cudaStream_t st) {
+    if (P.stream_mode != 1) throw StateError("no streaming analysis is open on this plan");
+    if (P.stream_pos >= P.S) {
+        P.stream_mode = 0;
+        return SFL_DONE;
+    }
+    const NSItem& it = P.items_host[P.stream_pos];
+    for (int ch = 0; ch < P.nch; ++ch)
+        analyze_items(P, P.X.as<float2>() + ch * P.H, reinterpret_cast<float*>(band) + ch, ZMap{}, P.nch,
+                      P.stream_pos, 1, false, st);
+    *index = it.s;
+    P.stream_pos += 1;
+    return SFL_OK;
+}
+
+void ns_stream_synth_begin(NSPlan& P, cudaStream_t) {
+    P.stream_mode = 2;
+    P.stream_pos = 0;
+}
+
+int ns_stream_synth_next_index(NSPlan& P, int* index) {
+    if (P.stream_mode != 2) throw StateError("no streaming synthesis is open on this plan");
+    if (P.stream_pos >= P.S) return SFL_DONE;
+    *index = P.items_host[P.stream_pos].s;
+    return SFL_OK;
+}
+
+void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
+    if (P.stream_mode != 2) throw StateError("no streaming synthesis is open on this plan");
+    if (P.stream_pos >= P.S) throw StateError("every subband has already been pushed");
+    for (int ch = 0; ch < P.nch; ++ch)
+        synth_items(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1, false,
+                    P.acc.as<float2>() + ch * P.H, P.comp.as<float2>() + ch * P.H, P.stream_pos == 0, st);
+    P.stream_pos += 1;
+}
+
+void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
+    if (P.stream_mode != 2 || P.stream_pos != P.S)
+        throw StateError("streaming synthesis ended before every subband was pushed");
+    for (int ch = 0; ch < P.nch; ++ch)
+        irfft3(P, P.acc.as<float2>() + ch * P.H, reinterpret_cast<float*>(x) + ch, P.nch, st);
+    P.stream_mode = 0;
+}
+
+}  // namespace sfl

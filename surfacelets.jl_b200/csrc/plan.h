@@ -1,0 +1,141 @@
+// Plan (workspace) state shared by the C ABI and the kernel drivers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "design.h"
+#include "fft_core.cuh"
+
+namespace sfl {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct AllocError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct StateError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void cuda_check(cudaError_t e, const char* what);
+
+// Device allocation owned by a plan.
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    DevMem(DevMem&& o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevMem& operator=(DevMem&& o) noexcept {
+        std::swap(p, o.p);
+        std::swap(bytes, o.bytes);
+        return *this;
+    }
+    ~DevMem();
+    void alloc(size_t n);
+    template <class T>
+    T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// Twiddle table and radix schedule of one FFT length, on the device.
+struct FFTLen {
+    FFTShape sh;
+    DevMem tw;
+};
+
+// Per-subband descriptor of the NS cascade (device copy in NSPlan::items).
+struct NSItem {
+    int s;        // 1-based subband index
+    int kind;     // 0 directional, 1 lowpass
+    int lv;       // pyramid level (0 = finest); the lowpass uses J
+    int i;        // hourglass 1..3
+    int wa_off, wb_off;    // float offsets of the two wedge planes
+    int wa_lo, wa_hi, wa_dlo;   // 0-based axes and lo extent of plane a
+    int wb_lo, wb_hi, wb_dlo;
+};
+
+// Offsets of the per-axis pyramid vectors and the table pointers.
+struct NSMaskTables {
+    const float* m1 = nullptr;
+    const float* m2 = nullptr;
+    const float* vec = nullptr;
+    const float* planes = nullptr;
+    int h1 = 0, n2 = 0, n3 = 0;
+    int tight = 1;
+    int pa_off[SFL_MAX_SCALES + 1][3] = {};
+    int pl_off[SFL_MAX_SCALES][3] = {};
+};
+
+struct NSPlan {
+    sfl_ns_params p{};
+    int dims[3] = {0, 0, 0};
+    int h1 = 0;
+    long long N = 0;      // voxels
+    long long H = 0;      // rfft grid points
+    int S = 0;            // subbands
+    int nch = 1;          // 1 real, 2 complex
+    int group = 8;
+    std::vector<NSItem> items_host;   // streaming / item order: directional ascending, then lowpass
+    DevMem items;
+    DevMem m1, m2, vec, planes;
+    NSMaskTables tb;
+    std::map<int, std::unique_ptr<FFTLen>> ffts;
+    DevMem X;        // nch spectra
+    DevMem work;     // group spectra
+    DevMem acc, comp;   // nch accumulators (+ Kahan compensation)
+    // streaming state
+    int stream_mode = 0;    // 0 idle, 1 analyzing, 2 synthesizing
+    int stream_pos = 0;
+    NSDesign design;        // kept for the table export
+};
+
+struct DecPlan;
+// DecPlan is complete only in dec.cu, which defines this deleter.
+struct DecPlanDeleter {
+    void operator()(DecPlan* d) const;
+};
+
+struct Plan {
+    int kind = SFL_KIND_NS;
+    int dtype = SFL_REAL32;
+    int device = 0;
+    std::unique_ptr<NSPlan> ns;
+    std::unique_ptr<DecPlan, DecPlanDeleter> dec;
+};
+
+// FFT length set-up (twiddles designed in float64).
+FFTLen* get_fft(std::map<int, std::unique_ptr<FFTLen>>& cache, int n);
+
+// NS drivers (ns.cu)
+void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype);
+void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
+void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
+void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);
+int ns_stream_analyze_next(NSPlan& P, void* band, int* index, cudaStream_t st);
+void ns_stream_synth_begin(NSPlan& P, cudaStream_t st);
+int ns_stream_synth_next_index(NSPlan& P, int* index);
+void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st);
+void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
+
+// Decimated drivers (dec.cu)
+void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], int dtype);
+int dec_nsubbands(const DecPlan& d);
+long long dec_ncoeffs(const DecPlan& d);
+void dec_subband_info(const DecPlan& d, int i, int shape[3], long long* offset);
+void dec_analyze(DecPlan& d, const void* x, void* c, cudaStream_t st);
+void dec_synthesize(DecPlan& d, const void* c, void* x, cudaStream_t st);
+void dec_adjoint_analyze(DecPlan& d, const void* c, void* x, cudaStream_t st);
+void dec_adjoint_synthesize(DecPlan& d, const void* x, void* c, cudaStream_t st);
+const SurfDesign& dec_design(const DecPlan& d);
+
+}  // namespace sfl

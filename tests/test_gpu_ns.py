@@ -1,0 +1,167 @@
+"""NSSurfacelet on the B200 through the C ABI, against the float64 oracle.
+
+Tolerances: rel. L2 <= 1e-5 of the whole coefficient set or volume against
+float64 (the float32 bar), the reference's own GPU-vs-CPU bound max|.| < 1e-4
+per subband (test/items/test_gpu.jl:51-218), and exact equality where the
+reference asserts it (complex = real + i imag, streaming = materialized).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+from oracle import ns as N
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+REL = 1e-5
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.complex128 if np.iscomplexobj(a) else np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(np.asarray(b).ravel()), 1e-300))
+
+
+def oracle_tables(dims, **kw):
+    return N.make_tables(N.NSParams.make(**kw), dims)
+
+
+CASES = [
+    ((16, 16, 16), dict(scales=2, direction_levels=[1, 2], bernstein_order=6)),
+    ((12, 20, 8), dict(scales=3, direction_levels=[1, 1, 2], bernstein_order=6)),
+    ((15, 20, 8), dict(scales=3, direction_levels=[1, 1, 2], bernstein_order=6)),
+    ((9, 7, 5), dict(scales=2, direction_levels=[1, 2], bernstein_order=6)),
+    ((32, 32, 32), dict(scales=3, direction_levels=[2, 2, 3])),
+    ((26, 30, 12), dict(scales=1, direction_levels=[3], bernstein_order=6, transition=0.5)),
+    ((16, 12, 20), dict(scales=2, direction_levels=[1, 2], bernstein_order=6, tight=False)),
+]
+
+
+@pytest.mark.parametrize("dims,kw", CASES)
+def test_analyze_synthesize_match_oracle(sfl, dims, kw):
+    rng = np.random.default_rng(202)
+    x = rng.standard_normal(dims).astype(np.float32)
+    t = sfl.NSSurfacelet(**kw)
+    T = oracle_tables(dims, **kw)
+    ws = sfl.make_workspace(t, "float32", dims)
+    xd = sfl.to_device(x)
+    c = sfl.analyze(t, xd, workspace=ws)
+    ch = sfl.to_host(c)
+    cref = N.analyze(T, x.astype(np.float64))
+    assert rel_l2(ch, cref) <= REL
+    for i in range(cref.shape[-1]):
+        assert np.abs(ch[..., i] - cref[..., i]).max() < 1e-4
+    r = sfl.to_host(sfl.synthesize(t, c, workspace=ws))
+    assert rel_l2(r, x) <= REL       # perfect reconstruction in float32
+    # synthesis of arbitrary coefficients against the oracle
+    cr = rng.standard_normal(cref.shape).astype(np.float32)
+    y = sfl.to_host(sfl.synthesize(t, sfl.to_device(cr), workspace=ws))
+    assert rel_l2(y, N.synthesize(T, cr.astype(np.float64))) <= REL
+
+
+@pytest.mark.parametrize("dims,kw", [CASES[0], CASES[2], CASES[6]])
+def test_adjoints(sfl, dims, kw):
+    rng = np.random.default_rng(7)
+    t = sfl.NSSurfacelet(**kw)
+    T = oracle_tables(dims, **kw)
+    ws = sfl.make_workspace(t, "float32", dims)
+    x = rng.standard_normal(dims).astype(np.float32)
+    c = rng.standard_normal(dims + (ws.nsubbands,)).astype(np.float32)
+    ax = sfl.to_host(sfl.adjoint_analyze(ws, sfl.to_device(c)))
+    assert rel_l2(ax, N.adjoint_analyze(T, c.astype(np.float64))) <= REL
+    sx = sfl.to_host(sfl.adjoint_synthesize(ws, sfl.to_device(x)))
+    assert rel_l2(sx, N.adjoint_synthesize(T, x.astype(np.float64))) <= REL
+    # <A x, c> = <x, A^T c>
+    Ax = sfl.to_host(sfl.analyze(ws, sfl.to_device(x))).astype(np.float64)
+    assert np.sum(Ax * c) == pytest.approx(np.sum(x.astype(np.float64) * ax), rel=1e-5)
+
+
+def test_parseval_and_constant(sfl):
+    # test/items/test_ns_surfacelet.jl:69-77, 218-237
+    dims = (16, 16, 16)
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[1, 1], bernstein_order=6)
+    x = np.random.default_rng(98).standard_normal(dims).astype(np.float32)
+    c = sfl.to_host(sfl.analyze(t, sfl.to_device(x))).astype(np.float64)
+    assert np.sum(c * c) == pytest.approx(np.sum(x.astype(np.float64) ** 2), rel=1e-5)
+    k = sfl.to_host(sfl.analyze(t, sfl.to_device(np.full(dims, 1.75, np.float32))))
+    assert np.abs(k[..., 0] - 1.75).max() < 1e-5
+    assert np.abs(k[..., 1:]).max() < 1e-5
+
+
+def test_complex_equals_real_plus_i_imag_bit_for_bit(sfl):
+    # test/items/test_ns_surfacelet.jl:140-152
+    dims = (16, 16, 16)
+    rng = np.random.default_rng(94)
+    xr = rng.standard_normal(dims).astype(np.float32)
+    xi = rng.standard_normal(dims).astype(np.float32)
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[1, 1], bernstein_order=6)
+    cc = sfl.to_host(sfl.analyze(t, sfl.to_device(xr + 1j * xi)))
+    cr = sfl.to_host(sfl.analyze(t, sfl.to_device(xr)))
+    ci = sfl.to_host(sfl.analyze(t, sfl.to_device(xi)))
+    assert np.array_equal(cc.real, cr) and np.array_equal(cc.imag, ci)
+    z = sfl.to_host(sfl.synthesize(t, sfl.to_device(cc)))
+    assert rel_l2(z, xr + 1j * xi) <= REL
+    yr = sfl.to_host(sfl.synthesize(t, sfl.to_device(cr)))
+    assert np.array_equal(z.real, yr)
+
+
+def test_streaming_matches_materialized(sfl):
+    # test/items/test_ns_surfacelet.jl:79-106
+    dims = (16, 16, 16)
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[1, 2], bernstein_order=6)
+    x = np.random.default_rng(92).standard_normal(dims).astype(np.float32)
+    ws = sfl.make_workspace(t, "float32", dims)
+    xd = sfl.to_device(x)
+    ref = sfl.analyze(ws, xd)
+    seen = []
+
+    def f(i, band):
+        seen.append(i)
+        assert bool((band == ref[..., i - 1]).all())
+
+    assert sfl.analyze(f, ws, xd) is None
+    assert seen == list(range(2, ws.nsubbands + 1)) + [1]
+    y = sfl.volume_like(dims)
+    assert sfl.synthesize_(lambda i: ref[..., i - 1], y, ws) is y
+    ym = sfl.synthesize(ws, ref)
+    assert bool((y == ym).all())
+    assert rel_l2(sfl.to_host(y), x) <= REL
+    with pytest.raises(sfl.DimensionMismatch):
+        sfl.synthesize_(lambda i: sfl.volume_like((4, 4, 4)), sfl.volume_like(dims), ws)
+
+
+def test_group_size_does_not_change_results(sfl):
+    dims = (20, 16, 12)
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[2, 3], bernstein_order=6)
+    x = sfl.to_device(np.random.default_rng(5).standard_normal(dims).astype(np.float32))
+    a = sfl.make_workspace(t, "float32", dims)
+    b = sfl.make_workspace(t, "float32", dims, group=3)
+    ca, cb = sfl.analyze(a, x), sfl.analyze(b, x)
+    assert bool((ca == cb).all())
+    assert bool((sfl.synthesize(a, ca) == sfl.synthesize(b, ca)).all())
+
+
+def test_workspace_validation(sfl):
+    # test/items/test_ns_surfacelet.jl:165-196
+    dims = (16, 16, 16)
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[1, 2], bernstein_order=6)
+    ws = sfl.make_workspace(t, "float32", dims)
+    x = sfl.to_device(np.zeros(dims, np.float32))
+    with pytest.raises(sfl.DimensionMismatch):
+        sfl.analyze(t, sfl.to_device(np.zeros((8, 8, 8), np.float32)), workspace=ws)
+    with pytest.raises(sfl.ArgumentError, match="element type"):
+        sfl.analyze(t, sfl.to_device(np.zeros(dims, np.complex64)), workspace=ws)
+    with pytest.raises(sfl.ArgumentError, match="the workspace was built for NSSurfacelet\\(scales = 1"):
+        sfl.analyze(t, x, workspace=sfl.make_workspace(sfl.NSSurfacelet(scales=1, direction_levels=[1]), "float32", dims))
+    with pytest.raises(sfl.DimensionMismatch):
+        sfl.analyze_(sfl.volume_like(dims + (5,)), t, x, workspace=ws)
+
+
+def test_host_arrays_round_trip(sfl):
+    # host (NumPy) arrays go through the same device path: the e2e form
+    dims = (12, 16, 10)
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[1, 2], bernstein_order=6)
+    x = np.asfortranarray(np.random.default_rng(13).standard_normal(dims).astype(np.float32))
+    c = sfl.analyze(t, x)
+    assert isinstance(c, np.ndarray) and c.shape == dims + (sfl.nsubbands(t, dims),)
+    assert rel_l2(sfl.synthesize(t, c), x) <= REL
