@@ -29,8 +29,8 @@ struct DecStageDev {
 struct DecLevelDev {
     int n[3], nlow[3];
     int cnt[3];
-    DevMem idx[3], idx_low[3], prof[3];
-    float invD15 = 1, D15 = 1;
+    DevMem idx[3], idx_low[3];
+    DevMem lw_split, lw_merge, hw;     // box weights (float64-designed)
     DevMem V[3];
     int hd[3][3];                     // [K][d] half-K dims
     std::vector<DecStageDev> stages[3];
@@ -70,10 +70,10 @@ __device__ __forceinline__ long long lin3(int a, int b, int c, int d0, int d1) {
 
 // src/pyramid/fourier_pyramid.jl:221-231 (file numbering): low = crop(L X)/D^1.5,
 // X[box] *= sqrt(1 - L^2).  `low` must be zeroed first.
+// lw[q] = L D^-1.5 and hw[q] = sqrt(1 - L^2) on the box, designed in float64.
 __global__ void pyr_split_kernel(float2* X, float2* low, int n0, int n1, int l0, int l1, const int* i0,
                                  const int* i1, const int* i2, const int* j0, const int* j1, const int* j2,
-                                 const float* p0, const float* p1, const float* p2, int c0, int c1, int c2,
-                                 float invD15) {
+                                 const float* lw, const float* hw, int c0, int c1, int c2) {
     long long total = (long long)c0 * c1 * c2;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x) {
@@ -81,19 +81,18 @@ __global__ void pyr_split_kernel(float2* X, float2* low, int n0, int n1, int l0,
         long long r = q / c0;
         int b = r % c1;
         int c = r / c1;
-        float L = p0[a] * p1[b] * p2[c];
         long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
         float2 v = X[xa];
-        low[lin3(j0[a], j1[b], j2[c], l0, l1)] = c_scale(v, L * invD15);
-        X[xa] = c_scale(v, sqrtf(1.f - L * L));
+        low[lin3(j0[a], j1[b], j2[c], l0, l1)] = c_scale(v, lw[q]);
+        X[xa] = c_scale(v, hw[q]);
     }
 }
 
 // src/pyramid/fourier_pyramid.jl:235-240: X[box] = sqrt(1-L^2) X[box] + L D^1.5 low.
+// lw[q] = L D^1.5 and hw[q] = sqrt(1 - L^2) on the box, designed in float64.
 __global__ void pyr_merge_kernel(float2* X, const float2* low, int n0, int n1, int l0, int l1, const int* i0,
                                  const int* i1, const int* i2, const int* j0, const int* j1, const int* j2,
-                                 const float* p0, const float* p1, const float* p2, int c0, int c1, int c2,
-                                 float D15) {
+                                 const float* lw, const float* hw, int c0, int c1, int c2) {
     long long total = (long long)c0 * c1 * c2;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
          q += (long long)gridDim.x * blockDim.x) {
@@ -101,10 +100,9 @@ __global__ void pyr_merge_kernel(float2* X, const float2* low, int n0, int n1, i
         long long r = q / c0;
         int b = r % c1;
         int c = r / c1;
-        float L = p0[a] * p1[b] * p2[c];
         long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
-        float2 h = c_scale(X[xa], sqrtf(1.f - L * L));
-        float2 w = c_scale(low[lin3(j0[a], j1[b], j2[c], l0, l1)], L * D15);
+        float2 h = c_scale(X[xa], hw[q]);
+        float2 w = c_scale(low[lin3(j0[a], j1[b], j2[c], l0, l1)], lw[q]);
         X[xa] = c_add(h, w);
     }
 }
@@ -298,12 +296,28 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
             L->cnt[d] = (int)pl.idx[d].size();
             upload_vec(L->idx[d], pl.idx[d]);
             upload_vec(L->idx_low[d], pl.idx_low[d]);
-            std::vector<float> pf(pl.prof[d].begin(), pl.prof[d].end());
-            upload_vec(L->prof[d], pf);
         }
-        double Dv = (double)pl.D.p / (double)pl.D.q;
-        L->D15 = (float)std::pow(Dv, 1.5);
-        L->invD15 = (float)(1.0 / (double)(float)std::pow(Dv, 1.5));
+        {
+            // src/pyramid/fourier_pyramid.jl:221-240 (file numbering): the
+            // separable lowpass L on the box, its D^-+1.5 scalings and
+            // sqrt(1 - L^2), in float64.
+            double Dv = (double)pl.D.p / (double)pl.D.q;
+            double D15 = std::pow(Dv, 1.5);
+            size_t nbox = (size_t)L->cnt[0] * L->cnt[1] * L->cnt[2];
+            std::vector<float> ls(nbox), lm(nbox), hw(nbox);
+            size_t q = 0;
+            for (int c = 0; c < L->cnt[2]; ++c)
+                for (int b = 0; b < L->cnt[1]; ++b)
+                    for (int a = 0; a < L->cnt[0]; ++a, ++q) {
+                        double Lv = pl.prof[0][a] * pl.prof[1][b] * pl.prof[2][c];
+                        ls[q] = (float)(Lv / D15);
+                        lm[q] = (float)(Lv * D15);
+                        hw[q] = (float)std::sqrt(1 - Lv * Lv);
+                    }
+            upload_vec(L->lw_split, ls);
+            upload_vec(L->lw_merge, lm);
+            upload_vec(L->hw, hw);
+        }
         int first = S.level_first[j];   // 0-based index of the level's first subband
         for (int K = 0; K < 3; ++K) {
             for (int d = 0; d < 3; ++d) L->hd[K][d] = d == K ? sc.n[K] / 2 + 1 : sc.n[d];
@@ -455,8 +469,8 @@ void pyr_split(DecPlan& D, int j, cudaStream_t st) {
         int tok = prof_begin("dec_pyr_split", st);
         pyr_split_kernel<<<grid_for(tot), 256, 0, st>>>(
             X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
-            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.prof[0].as<float>(),
-            L.prof[1].as<float>(), L.prof[2].as<float>(), L.cnt[0], L.cnt[1], L.cnt[2], L.invD15);
+            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.lw_split.as<float>(),
+            L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
         prof_end(tok, st);
     }
     cuda_check(cudaGetLastError(), "pyr_split_kernel");
@@ -471,8 +485,8 @@ void pyr_merge(DecPlan& D, int j, cudaStream_t st) {
         int tok = prof_begin("dec_pyr_merge", st);
         pyr_merge_kernel<<<grid_for(tot), 256, 0, st>>>(
             X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
-            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.prof[0].as<float>(),
-            L.prof[1].as<float>(), L.prof[2].as<float>(), L.cnt[0], L.cnt[1], L.cnt[2], L.D15);
+            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.lw_merge.as<float>(),
+            L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
         prof_end(tok, st);
     }
     cuda_check(cudaGetLastError(), "pyr_merge_kernel");

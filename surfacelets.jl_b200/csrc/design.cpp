@@ -382,6 +382,31 @@ NSDesign ns_design(const sfl_ns_params& p, const int dims[3]) {
     return D;
 }
 
+// src/transforms/ns_surfacelet.jl:265-272 (_hg_factor, _bandpass), 278-303
+std::vector<double> ns_group_mask(const NSDesign& D, int lv, int i, bool hourglass) {
+    const int h1 = D.h1, n2 = D.dims[1], n3 = D.dims[2];
+    std::vector<double> G((size_t)h1 * n2 * n3);
+    const auto& a = D.pa[lv];
+    const auto& l = D.pl[lv];
+    for (int k3 = 0; k3 < n3; ++k3)
+        for (int k2 = 0; k2 < n2; ++k2)
+            for (int k1 = 0; k1 < h1; ++k1) {
+                size_t q = k1 + (size_t)h1 * (k2 + (size_t)n2 * k3);
+                double L = l[0][k1] * l[1][k2] * l[2][k3];
+                double B = a[0][k1] * a[1][k2] * a[2][k3] * std::sqrt(std::max(1 - L * L, 0.0));
+                if (!hourglass) {
+                    G[q] = B;
+                    continue;
+                }
+                double f1 = D.m1[q], f2 = D.m2[k2 + (size_t)n2 * k3];
+                double w1 = i == 1 ? f1 : 1 - f1;
+                double w2 = i == 1 ? 1.0 : (i == 2 ? f2 : 1 - f2);
+                double w = w1 * w2;
+                G[q] = B * (D.p.tight ? std::sqrt(std::max(w, 0.0)) : w);
+            }
+    return G;
+}
+
 // ── Decimated Surfacelet ──────────────────────────────────────────────────────
 
 // src/types/transforms.jl:270-278 with the wedge split of ndfb_wedges.jl:19

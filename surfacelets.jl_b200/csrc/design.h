@@ -66,6 +66,13 @@ struct NSDesign {
     std::vector<std::array<std::vector<double>, 3>> pa, pl;
 };
 
+// Group mask of hourglass i (1..3) at pyramid level lv on the rfft grid:
+// B_lv * sqrt(max(W_i, 0)) when tight, B_lv * W_i otherwise; with
+// hourglass = false, B_lv alone.  Float64 throughout: in float32 the
+// cancellations in 1 - (l1 l2 l3)^2 and 1 - f0 cost up to 1.5e-4 absolute
+// after the square root.
+std::vector<double> ns_group_mask(const NSDesign& D, int lv, int i, bool hourglass);
+
 void ns_check_params(const sfl_ns_params& p);
 void ns_check_size(const sfl_ns_params& p, const int dims[3]);
 int ns_nbands(const sfl_ns_params& p, int j);      // scale j 1-based

@@ -10,9 +10,10 @@
 //     every subband of a group in one CTA and accumulates M_s * F_s in
 //     registers with Kahan compensation; one accumulator round trip per group.
 //
-// M_s = B_j * hg_i * w_a * w_b is evaluated per element from the float32
-// tables (m1 on the grid, m2 and the wedge planes on planes, the pyramid
-// factors on axes), never materialized.
+// M_s = (B_j hg_i) * w_a * w_b is evaluated per element from float32 tables
+// designed in float64: the group factor B_j hg_i on the rfft grid (one table
+// per scale and hourglass) and the wedge planes; M_s itself is never
+// materialized.
 #include <cmath>
 #include <cstring>
 
@@ -21,34 +22,26 @@
 
 namespace sfl {
 
-// Mask of item `it` at rfft-grid point (k1, k2, k3).  synth selects the
-// synthesis mask, which is B_j alone when the bank is not tight
-// (src/transforms/ns_surfacelet.jl:226-227, 237-238).
+// Mask of item `it` at rfft-grid point (k1, k2, k3), linear index q.  synth
+// selects the synthesis mask, which is B_j alone when the bank is not tight
+// (src/transforms/ns_surfacelet.jl:226-227, 237-238).  The group factor
+// B_j hg_i comes from a float64-designed table; the wedge planes are
+// square-rooted in float64 too, so only well-conditioned float32 products
+// remain here.
 __device__ __forceinline__ float ns_mask(const NSMaskTables& tb, const NSItem& it, int k1, int k2, int k3,
-                                         bool synth) {
-    const float* v = tb.vec;
-    const int L = it.lv;
+                                         long long q, bool synth) {
     if (it.kind == 1) {
         // lowpass a1 a2 a3: src/transforms/ns_surfacelet.jl:358-371
-        return v[tb.pa_off[L][0] + k1] * v[tb.pa_off[L][1] + k2] * v[tb.pa_off[L][2] + k3];
+        const float* v = tb.vec;
+        return v[tb.low_off[0] + k1] * v[tb.low_off[1] + k2] * v[tb.low_off[2] + k3];
     }
-    // B_j: src/transforms/ns_surfacelet.jl:271-272
-    float a = v[tb.pa_off[L][0] + k1] * v[tb.pa_off[L][1] + k2] * v[tb.pa_off[L][2] + k3];
-    float l = v[tb.pl_off[L][0] + k1] * v[tb.pl_off[L][1] + k2] * v[tb.pl_off[L][2] + k3];
-    float B = a * sqrtf(fmaxf(1.f - l * l, 0.f));
-    if (synth && !tb.tight) return B;
-    // hourglass factor: src/transforms/ns_surfacelet.jl:265-268, hourglass.jl:289-303
-    float f1 = tb.m1[k1 + (long long)tb.h1 * (k2 + (long long)tb.n2 * k3)];
-    float f2 = tb.m2[k2 + (long long)tb.n2 * k3];
-    float w1 = it.i == 1 ? f1 : 1.f - f1;
-    float w2 = it.i == 1 ? 1.f : (it.i == 2 ? f2 : 1.f - f2);
-    float w = w1 * w2;
-    float hg = tb.tight ? sqrtf(fmaxf(w, 0.f)) : w;
+    if (synth && !tb.tight) return tb.Bl[(long long)it.lv * tb.H + q];
+    float G = tb.G[(long long)it.g * tb.H + q];
     // wedge planes: src/transforms/ns_surfacelet.jl:376-427
     int kk[3] = {k1, k2, k3};
     float wa = tb.planes[it.wa_off + kk[it.wa_lo] + it.wa_dlo * kk[it.wa_hi]];
     float wb = tb.planes[it.wb_off + kk[it.wb_lo] + it.wb_dlo * kk[it.wb_hi]];
-    return ((B * hg) * wa) * wb;
+    return (G * wa) * wb;
 }
 
 // Pass-3 load of the analysis: lines along axis 3 of X, times the mask of
@@ -71,7 +64,8 @@ struct LoadNSMask {
             float2 v = make_float2(0.f, 0.f);
             if (l < nlines) {
                 int k1 = l % tb.h1, k2 = l / tb.h1;
-                v = c_scale(X[l + (long long)i * si], ns_mask(tb, it, k1, k2, i, synth != 0));
+                long long q = l + (long long)i * si;
+                v = c_scale(X[q], ns_mask(tb, it, k1, k2, i, q, synth != 0));
             }
             tile[t * npad + i] = v;
         }
@@ -132,7 +126,7 @@ __global__ void __launch_bounds__(256) ns_accum_kernel(const float2* __restrict_
                 int t = idx % T, i = idx / T, l = l0 + t;
                 if (l < nlines) {
                     int k1 = l % tb.h1, k2 = l / tb.h1;
-                    float m = ns_mask(tb, it, k1, k2, i, synth != 0);
+                    float m = ns_mask(tb, it, k1, k2, i, l + (long long)i * si, synth != 0);
                     float2 v = c_scale(r[t * npad + i], m);
                     // Kahan: y = v - c ; t = s + y ; c = (t - s) - y ; s = t
                     float2 y = c_sub(v, c[e]);
@@ -225,21 +219,30 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     P.nch = dtype == SFL_COMPLEX64 ? 2 : 1;
     const int J = p.scales;
 
-    // tables
-    upload(P.m1, to_f32(D.m1));
-    upload(P.m2, to_f32(D.m2));
-    std::vector<float> vec;
+    // tables: group masks (and level bandpasses when not tight), designed in float64
     NSMaskTables& tb = P.tb;
-    for (int lv = 0; lv <= J; ++lv)
-        for (int d = 0; d < 3; ++d) {
-            tb.pa_off[lv][d] = (int)vec.size();
-            for (double x : D.pa[lv][d]) vec.push_back((float)x);
-        }
-    for (int lv = 0; lv < J; ++lv)
-        for (int d = 0; d < 3; ++d) {
-            tb.pl_off[lv][d] = (int)vec.size();
-            for (double x : D.pl[lv][d]) vec.push_back((float)x);
-        }
+    {
+        std::vector<float> G;
+        G.reserve((size_t)3 * J * P.H);
+        for (int j = 1; j <= J; ++j)
+            for (int i = 1; i <= 3; ++i) {
+                std::vector<double> g = ns_group_mask(D, J - j, i, true);
+                for (double v : g) G.push_back((float)v);
+            }
+        upload(P.G, G);
+        std::vector<float> Bl;
+        if (!p.tight)
+            for (int lv = 0; lv < J; ++lv) {
+                std::vector<double> b = ns_group_mask(D, lv, 1, false);
+                for (double v : b) Bl.push_back((float)v);
+            }
+        upload(P.Bl, Bl);
+    }
+    std::vector<float> vec;
+    for (int d = 0; d < 3; ++d) {
+        tb.low_off[d] = (int)vec.size();
+        for (double x : D.pa[J][d]) vec.push_back((float)x);
+    }
     upload(P.vec, vec);
     std::vector<float> planes;
     // plane_off[j][i][plane][w]
@@ -254,8 +257,9 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
                 }
             }
     upload(P.planes, planes);
-    tb.m1 = P.m1.as<float>();
-    tb.m2 = P.m2.as<float>();
+    tb.G = P.G.as<float>();
+    tb.Bl = P.Bl.as<float>();
+    tb.H = P.H;
     tb.vec = P.vec.as<float>();
     tb.planes = P.planes.as<float>();
     tb.h1 = P.h1;
@@ -278,6 +282,7 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
                     it.kind = 0;
                     it.lv = J - j;
                     it.i = i;
+                    it.g = 3 * (j - 1) + (i - 1);
                     const WedgePlanes& Wa = D.wedges[j - 1][i - 1][0];
                     const WedgePlanes& Wb = D.wedges[j - 1][i - 1][1];
                     it.wa_off = off[j - 1][i - 1][0][a - 1];

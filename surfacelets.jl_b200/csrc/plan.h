@@ -59,21 +59,24 @@ struct NSItem {
     int kind;     // 0 directional, 1 lowpass
     int lv;       // pyramid level (0 = finest); the lowpass uses J
     int i;        // hourglass 1..3
+    int g;        // group (scale, hourglass): index of its mask table
     int wa_off, wb_off;    // float offsets of the two wedge planes
     int wa_lo, wa_hi, wa_dlo;   // 0-based axes and lo extent of plane a
     int wb_lo, wb_hi, wb_dlo;
 };
 
-// Offsets of the per-axis pyramid vectors and the table pointers.
+// Mask tables on the device: the group masks (float64-designed, one rfft
+// grid each), the level bandpasses (synthesis of a bank that is not tight),
+// the lowpass's per-axis factors and the wedge planes.
 struct NSMaskTables {
-    const float* m1 = nullptr;
-    const float* m2 = nullptr;
-    const float* vec = nullptr;
+    const float* G = nullptr;       // [group][H]
+    const float* Bl = nullptr;      // [level][H] (not tight only)
+    const float* vec = nullptr;     // lowpass factors a1 | a2 | a3
     const float* planes = nullptr;
+    long long H = 0;
     int h1 = 0, n2 = 0, n3 = 0;
     int tight = 1;
-    int pa_off[SFL_MAX_SCALES + 1][3] = {};
-    int pl_off[SFL_MAX_SCALES][3] = {};
+    int low_off[3] = {0, 0, 0};
 };
 
 struct NSPlan {
@@ -87,7 +90,7 @@ struct NSPlan {
     int group = 8;
     std::vector<NSItem> items_host;   // streaming / item order: directional ascending, then lowpass
     DevMem items;
-    DevMem m1, m2, vec, planes;
+    DevMem G, Bl, vec, planes;
     NSMaskTables tb;
     std::map<int, std::unique_ptr<FFTLen>> ffts;
     DevMem X;        // nch spectra
