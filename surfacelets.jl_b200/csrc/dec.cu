@@ -18,6 +18,7 @@
 
 #include "passes.cuh"
 #include "plan.h"
+#include "regpass.cuh"
 
 namespace sfl {
 
@@ -204,6 +205,7 @@ struct BlockMap {
     int ba, bb, ca;    // block sizes along a, b; block count along a
     long long first, blk;
     int sd0, sd1;      // subband dims along axes 0, 1
+    long long sK;      // element stride of axis K inside a subband
     __device__ __forceinline__ long long addr(int l, int i) const {
         int c_a = l % ha, c_b = l / ha;
         int pa = c_a / ba, ra = c_a - pa * ba;
@@ -265,6 +267,45 @@ struct LoadRPairBlocks {
             float b = la + 1 < nlines ? src[bm.addr(la + 1, i) * es] : 0.f;
             tile[t * npad + i] = make_float2(a, b);
         }
+    }
+};
+
+// Register-pass versions of the two block ops (see regpass.cuh).
+struct RStoreRPairBlocks {
+    static constexpr bool kStaged = false;
+    float* dst;
+    BlockMap bm;
+    int nlines;
+    int es;
+    struct Ctx {
+        long long a, b;
+    };
+    __device__ __forceinline__ Ctx line(int, int l, bool valid) const {
+        int la = 2 * l;
+        return Ctx{valid && la < nlines ? bm.addr(la, 0) : -1, valid && la + 1 < nlines ? bm.addr(la + 1, 0) : -1};
+    }
+    __device__ __forceinline__ void put(const Ctx& c, int k, float2 v) const {
+        if (c.a >= 0) dst[(c.a + k * bm.sK) * es] = v.x;
+        if (c.b >= 0) dst[(c.b + k * bm.sK) * es] = v.y;
+    }
+};
+
+struct RLoadRPairBlocks {
+    const float* src;
+    BlockMap bm;
+    int nlines;
+    int es;
+    struct Ctx {
+        long long a, b;
+    };
+    __device__ __forceinline__ Ctx line(int, int l, bool valid) const {
+        int la = 2 * l;
+        return Ctx{valid && la < nlines ? bm.addr(la, 0) : -1, valid && la + 1 < nlines ? bm.addr(la + 1, 0) : -1};
+    }
+    __device__ __forceinline__ float2 get(const Ctx& c, int i) const {
+        float a = c.a >= 0 ? src[(c.a + i * bm.sK) * es] : 0.f;
+        float b = c.b >= 0 ? src[(c.b + i * bm.sK) * es] : 0.f;
+        return make_float2(a, b);
     }
 };
 
@@ -378,12 +419,19 @@ unsigned grid_for(long long total) {
 void fft_real_full(DecPlan& D, const float* x, int es, const int d[3], float2* X, cudaStream_t st) {
     Lines gin = axis_lines(d, 0);
     FFTLen* f0 = get_fft(D.ffts, d[0]);
-    LoadRPair ld{x, ZMap{}, gin, es};
-    StoreFullPair sto{X, ZMap{}, gin};
-    launch_pass(ld, sto, f0->sh, (gin.nlines + 1) / 2, 1, false, st, "dec_fft_r2c");
+    int pairs = (gin.nlines + 1) / 2;
+    if (!launch_reg<false>(d[0], RLoadRPair{x, ZMap{}, gin, es}, RStoreFullPair{X, ZMap{}, gin, d[0]}, f0->sh.tw,
+                           pairs, 1, false, st, "dec_fft_r2c")) {
+        LoadRPair ld{x, ZMap{}, gin, es};
+        StoreFullPair sto{X, ZMap{}, gin};
+        launch_pass(ld, sto, f0->sh, pairs, 1, false, st, "dec_fft_r2c");
+    }
     for (int a = 1; a < 3; ++a) {
         Lines g = axis_lines(d, a);
         FFTLen* f = get_fft(D.ffts, d[a]);
+        if (launch_reg<false>(d[a], RLoadC{X, ZMap{}, g}, RStoreC{X, ZMap{}, g}, f->sh.tw, g.nlines, 1, true, st,
+                              "dec_fft_c2c"))
+            continue;
         LoadC l2{X, ZMap{}, g, 1.f};
         StoreC s2{X, ZMap{}, g, 1.f};
         launch_pass(l2, s2, f->sh, g.nlines, 1, false, st, "dec_fft_c2c");
@@ -395,12 +443,18 @@ void ifft_full_real(DecPlan& D, float2* X, const int d[3], float* out, int es, f
     for (int a = 2; a >= 1; --a) {
         Lines g = axis_lines(d, a);
         FFTLen* f = get_fft(D.ffts, d[a]);
+        if (launch_reg<true>(d[a], RLoadC{X, ZMap{}, g}, RStoreC{X, ZMap{}, g}, f->sh.tw, g.nlines, 1, true, st,
+                             "dec_fft_c2c"))
+            continue;
         LoadC l2{X, ZMap{}, g, 1.f};
         StoreC s2{X, ZMap{}, g, 1.f};
         launch_pass(l2, s2, f->sh, g.nlines, 1, true, st, "dec_fft_c2c");
     }
     Lines g0 = axis_lines(d, 0);
     FFTLen* f0 = get_fft(D.ffts, d[0]);
+    if (launch_reg<true>(d[0], RLoadC{X, ZMap{}, g0}, RStoreReal{out, ZMap{}, g0, es, scale}, f0->sh.tw, g0.nlines,
+                         1, false, st, "dec_fft_real"))
+        return;
     LoadC l0{X, ZMap{}, g0, 1.f};
     StoreReal s0{out, ZMap{}, g0, es, scale};
     launch_pass(l0, s0, f0->sh, g0.nlines, 1, true, st, "dec_fft_real");
@@ -421,6 +475,12 @@ void block_fft(DecPlan& D, float2* S, const int hd[3], int m, int bl, bool inv, 
     g.si = str[m];
     g.nlines = hd[o[0]] * hd[o[1]] * (hd[m] / bl);
     FFTLen* f = get_fft(D.ffts, bl);
+    bool tf = g.si != 1;
+    bool done = inv ? launch_reg<true>(bl, RLoadC{S, ZMap{}, g}, RStoreC{S, ZMap{}, g}, f->sh.tw, g.nlines, 1, tf, st,
+                                       "dec_block_fft")
+                    : launch_reg<false>(bl, RLoadC{S, ZMap{}, g}, RStoreC{S, ZMap{}, g}, f->sh.tw, g.nlines, 1, tf,
+                                        st, "dec_block_fft");
+    if (done) return;
     LoadC ld{S, ZMap{}, g, 1.f};
     StoreC sto{S, ZMap{}, g, 1.f};
     launch_pass(ld, sto, f->sh, g.nlines, 1, inv, st, "dec_block_fft");
@@ -441,6 +501,7 @@ BlockMap block_map(const DecLevelDev& L, int K) {
     for (int d = 0; d < 3; ++d) sd[d] = d == K ? L.n[K] : L.bsize[K][d];
     bm.sd0 = sd[0];
     bm.sd1 = sd[1];
+    bm.sK = K == 0 ? 1 : (K == 1 ? (long long)sd[0] : (long long)sd[0] * sd[1]);
     return bm;
 }
 
@@ -522,9 +583,14 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
             if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], true, st);
         Lines gk = k_lines(L, K);
         FFTLen* f = get_fft(D.ffts, L.n[K]);
-        LoadHPair ld{S, ZMap{}, gk};
-        StoreRPairBlocks sto{c, block_map(L, K), gk.nlines, es};
-        launch_pass(ld, sto, f->sh, (gk.nlines + 1) / 2, 1, true, st, "dec_c2r_blocks");
+        BlockMap bm = block_map(L, K);
+        int pairs = (gk.nlines + 1) / 2;
+        if (!launch_reg<true>(L.n[K], RLoadHPair{S, ZMap{}, gk, L.n[K]}, RStoreRPairBlocks{c, bm, gk.nlines, es},
+                              f->sh.tw, pairs, 1, K != 0, st, "dec_c2r_blocks")) {
+            LoadHPair ld{S, ZMap{}, gk};
+            StoreRPairBlocks sto{c, bm, gk.nlines, es};
+            launch_pass(ld, sto, f->sh, pairs, 1, true, st, "dec_c2r_blocks");
+        }
     }
 }
 
@@ -536,9 +602,14 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
         float2* S = D.S[K].as<float2>();
         Lines gk = k_lines(L, K);
         FFTLen* f = get_fft(D.ffts, L.n[K]);
-        LoadRPairBlocks ld{c, block_map(L, K), gk.nlines, es};
-        StoreHalfPair sto{S, ZMap{}, gk};
-        launch_pass(ld, sto, f->sh, (gk.nlines + 1) / 2, 1, false, st, "dec_r2c_blocks");
+        BlockMap bm = block_map(L, K);
+        int pairs = (gk.nlines + 1) / 2;
+        if (!launch_reg<false>(L.n[K], RLoadRPairBlocks{c, bm, gk.nlines, es}, RStoreHalfPair{S, ZMap{}, gk, L.n[K]},
+                               f->sh.tw, pairs, 1, K != 0, st, "dec_r2c_blocks")) {
+            LoadRPairBlocks ld{c, bm, gk.nlines, es};
+            StoreHalfPair sto{S, ZMap{}, gk};
+            launch_pass(ld, sto, f->sh, pairs, 1, false, st, "dec_r2c_blocks");
+        }
         for (int m = 0; m < 3; ++m)
             if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
         long long tot = (long long)hd[0] * hd[1] * hd[2];

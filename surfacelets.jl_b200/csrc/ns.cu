@@ -19,6 +19,7 @@
 
 #include "passes.cuh"
 #include "plan.h"
+#include "regpass.cuh"
 
 namespace sfl {
 
@@ -149,6 +150,166 @@ __global__ void __launch_bounds__(256) ns_accum_kernel(const float2* __restrict_
             }
         }
     }
+}
+
+// Per-line mask context of an NS item for lines along axis 3 (line l =
+// (k1, k2), element k3): mask(k3) = m[k3 * si] * wa(k3) * wb(k3), each plane
+// either constant along the line or stepping with k3.
+struct NSMaskLine {
+    const float* m;       // group table (or level bandpass) at the line's first point
+    const float* wa;
+    const float* wb;
+    int was, wbs;         // steps of the planes along k3 (0: constant)
+    int plain;            // 1: the mask is m alone (bandpass of an untight synthesis)
+    int low;              // 1: lowpass a1 a2 a3
+    float lowc;           // a1[k1] a2[k2]
+    const float* lowv;    // a3
+};
+
+__device__ __forceinline__ NSMaskLine ns_mask_line(const NSMaskTables& tb, const NSItem& it, int l, bool synth) {
+    NSMaskLine c;
+    const int k1 = l % tb.h1, k2 = l / tb.h1;
+    c.low = it.kind == 1;
+    c.plain = 0;
+    c.m = nullptr;
+    c.wa = c.wb = nullptr;
+    c.was = c.wbs = 0;
+    c.lowc = 0.f;
+    c.lowv = nullptr;
+    if (c.low) {
+        c.lowc = tb.vec[tb.low_off[0] + k1] * tb.vec[tb.low_off[1] + k2];
+        c.lowv = tb.vec + tb.low_off[2];
+        return c;
+    }
+    if (synth && !tb.tight) {
+        c.plain = 1;
+        c.m = tb.Bl + (long long)it.lv * tb.H + l;
+        return c;
+    }
+    c.m = tb.G + (long long)it.g * tb.H + l;
+    const int kk[3] = {k1, k2, 0};
+    // a plane over (lo, hi): index off + k_lo + dlo * k_hi; axis 3 can only be hi
+    c.wa = tb.planes + it.wa_off + kk[it.wa_lo] + (it.wa_hi == 2 ? 0 : it.wa_dlo * kk[it.wa_hi]);
+    c.was = it.wa_hi == 2 ? it.wa_dlo : 0;
+    c.wb = tb.planes + it.wb_off + kk[it.wb_lo] + (it.wb_hi == 2 ? 0 : it.wb_dlo * kk[it.wb_hi]);
+    c.wbs = it.wb_hi == 2 ? it.wb_dlo : 0;
+    return c;
+}
+
+__device__ __forceinline__ float ns_mask_at(const NSMaskLine& c, int k3, long long si) {
+    if (c.low) return c.lowc * c.lowv[k3];
+    float g = c.m[(long long)k3 * si];
+    if (c.plain) return g;
+    return (g * c.wa[k3 * c.was]) * c.wb[k3 * c.wbs];
+}
+
+// Analysis pass-3 load for the register kernel: X times the mask of item z.
+struct RLoadNSMask {
+    const float2* X;
+    NSMaskTables tb;
+    const NSItem* items;
+    int item0;
+    int synth;
+    struct Ctx {
+        const float2* x;
+        NSMaskLine m;
+        long long si;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const {
+        Ctx c;
+        c.si = (long long)tb.h1 * tb.n2;
+        c.x = X + (valid ? l : 0);
+        c.m = ns_mask_line(tb, items[item0 + z], valid ? l : 0, synth != 0);
+        return c;
+    }
+    __device__ __forceinline__ float2 get(const Ctx& c, int i) const {
+        return c_scale(c.x[i * c.si], ns_mask_at(c.m, i, c.si));
+    }
+};
+
+// Synthesis pass 3 on the register FFT: every item of the group is
+// transformed along axis 3 and accumulated (Kahan) in registers.
+template <int N>
+__global__ void __launch_bounds__(256) ns_accum_reg_kernel(const float2* __restrict__ work, long long H, int G,
+                                                           NSMaskTables tb, const NSItem* __restrict__ items,
+                                                           int item0, int synth, float2* acc, float2* comp, int init,
+                                                           const float2* __restrict__ tw, int nlines) {
+    using Ge = RegGeom<N>;
+    constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
+    extern __shared__ float2 xch[];
+    const int tid = threadIdx.x;
+    const int lp = tid % LP, p = tid / LP;
+    const int l = blockIdx.x * LP + lp;
+    const bool valid = l < nlines;
+    const long long si = (long long)tb.h1 * tb.n2;
+    float2* xl = xch + lp * Ge::XLINE;
+    float2 s[E], c[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        s[e] = make_float2(0.f, 0.f);
+        c[e] = make_float2(0.f, 0.f);
+    }
+    if (!init && valid) {
+#pragma unroll
+        for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+            for (int k = 0; k < N2; ++k) {
+                long long q = l + (long long)((p + N2 * j) + N1 * k) * si;
+                s[j * N2 + k] = acc[q];
+                c[j * N2 + k] = comp[q];
+            }
+    }
+    for (int z = 0; z < G; ++z) {
+        RLoadC ld{work + (long long)z * H, ZMap{}, Lines{}};
+        ld.g.si = si;
+        RLoadC::Ctx lc{ld.src + (valid ? l : 0)};
+        float2 u[E];
+        reg_line_fft<N, false>(ld, lc, valid, p, xl, tw, u);
+        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], valid ? l : 0, synth != 0);
+#pragma unroll
+        for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+            for (int k = 0; k < N2; ++k) {
+                const int k3 = (p + N2 * j) + N1 * k;
+                float2 v = c_scale(u[j * N2 + k], ns_mask_at(mk, k3, si));
+                const int e = j * N2 + k;
+                float2 y = c_sub(v, c[e]);
+                float2 t = c_add(s[e], y);
+                c[e] = c_sub(c_sub(t, s[e]), y);
+                s[e] = t;
+            }
+        __syncthreads();   // the exchange rows are reused by the next item
+    }
+    if (valid) {
+#pragma unroll
+        for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+            for (int k = 0; k < N2; ++k) {
+                long long q = l + (long long)((p + N2 * j) + N1 * k) * si;
+                acc[q] = s[j * N2 + k];
+                comp[q] = c[j * N2 + k];
+            }
+    }
+}
+
+template <int N>
+static void launch_accum_reg(const float2* W, long long H, int nz, const NSMaskTables& tb, const NSItem* items,
+                             int i0, int synth, float2* acc, float2* comp, int init, const float2* tw, int nlines,
+                             cudaStream_t st) {
+    using Ge = RegGeom<N>;
+    static bool configured = false;
+    if (!configured) {
+        cuda_check(cudaFuncSetAttribute(ns_accum_reg_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Ge::SMEM),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    dim3 grid((nlines + Ge::LP - 1) / Ge::LP);
+    int tok = prof_begin("ns_accum_axis3", st);
+    ns_accum_reg_kernel<N><<<grid, Ge::THREADS, Ge::SMEM, st>>>(W, H, nz, tb, items, i0, synth, acc, comp, init, tw,
+                                                                nlines);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "ns_accum_reg_kernel launch");
 }
 
 // ── set-up ───────────────────────────────────────────────────────────────────
@@ -335,11 +496,15 @@ void pass_r2c(NSPlan& P, const float* src, ZMap zin, int es, float2* dst, long l
     Lines gin = axis_lines(P.dims, 0);
     Grid hg = half_grid(P);
     Lines gout = axis_lines(hg.d, 0);
-    LoadRPair ld{src, zin, gin, es};
     ZMap zo;
     zo.zstride = dst_zstride;
+    int pairs = (gin.nlines + 1) / 2;
+    if (launch_reg<false>(f->sh.n, RLoadRPair{src, zin, gin, es}, RStoreHalfPair{dst, zo, gout, f->sh.n}, f->sh.tw,
+                          pairs, nz, false, st, "ns_r2c_axis1"))
+        return;
+    LoadRPair ld{src, zin, gin, es};
     StoreHalfPair sto{dst, zo, gout};
-    launch_pass(ld, sto, f->sh, (gin.nlines + 1) / 2, nz, false, st, "ns_r2c_axis1");
+    launch_pass(ld, sto, f->sh, pairs, nz, false, st, "ns_r2c_axis1");
 }
 
 // C2R along axis 1 of nz spectra into nz real volumes, scaled.
@@ -351,9 +516,13 @@ void pass_c2r(NSPlan& P, const float2* src, long long src_zstride, float* dst, Z
     Lines gout = axis_lines(P.dims, 0);
     ZMap zi;
     zi.zstride = src_zstride;
+    int pairs = (gout.nlines + 1) / 2;
+    if (launch_reg<true>(f->sh.n, RLoadHPair{src, zi, gin, f->sh.n}, RStoreRPair{dst, zout, gout, es, scale},
+                         f->sh.tw, pairs, nz, false, st, "ns_c2r_axis1"))
+        return;
     LoadHPair ld{src, zi, gin};
     StoreRPair sto{dst, zout, gout, es, scale};
-    launch_pass(ld, sto, f->sh, (gout.nlines + 1) / 2, nz, true, st, "ns_c2r_axis1");
+    launch_pass(ld, sto, f->sh, pairs, nz, true, st, "ns_c2r_axis1");
 }
 
 // Complex FFT along axis a (1 or 2, 0-based) of nz spectra.
@@ -364,9 +533,16 @@ void pass_c2c(NSPlan& P, const float2* src, float2* dst, long long zstride, int 
     Lines g = axis_lines(hg.d, axis);
     ZMap zm;
     zm.zstride = zstride;
+    const char* tag = axis == 1 ? "ns_c2c_axis2" : "ns_c2c_axis3";
+    bool tf = g.si != 1;
+    bool done = inv ? launch_reg<true>(f->sh.n, RLoadC{src, zm, g}, RStoreC{dst, zm, g}, f->sh.tw, g.nlines, nz, tf,
+                                       st, tag)
+                    : launch_reg<false>(f->sh.n, RLoadC{src, zm, g}, RStoreC{dst, zm, g}, f->sh.tw, g.nlines, nz,
+                                        tf, st, tag);
+    if (done) return;
     LoadC ld{src, zm, g, 1.f};
     StoreC sto{dst, zm, g, 1.f};
-    launch_pass(ld, sto, f->sh, g.nlines, nz, inv, st, axis == 1 ? "ns_c2c_axis2" : "ns_c2c_axis3");
+    launch_pass(ld, sto, f->sh, g.nlines, nz, inv, st, tag);
 }
 
 // The coefficient subbands of items [i0, ...): subband s at (s-1)*N*es.
@@ -398,12 +574,15 @@ void analyze_items(NSPlan& P, const float2* X, float* cbase, ZMap zc, int es, in
     float2* W = P.work.as<float2>();
     Grid hg = half_grid(P);
     FFTLen* f3 = get_fft(P.ffts, P.dims[2]);
-    LoadNSMask ld{X, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0};
     Lines g3 = axis_lines(hg.d, 2);
     ZMap zw;
     zw.zstride = P.H;
-    StoreC sto{W, zw, g3, 1.f};
-    launch_pass(ld, sto, f3->sh, g3.nlines, nz, true, st, "ns_mask_axis3");
+    if (!launch_reg<true>(f3->sh.n, RLoadNSMask{X, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0},
+                          RStoreC{W, zw, g3}, f3->sh.tw, g3.nlines, nz, true, st, "ns_mask_axis3")) {
+        LoadNSMask ld{X, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0};
+        StoreC sto{W, zw, g3, 1.f};
+        launch_pass(ld, sto, f3->sh, g3.nlines, nz, true, st, "ns_mask_axis3");
+    }
     pass_c2c(P, W, W, P.H, 1, true, nz, st);
     pass_c2r(P, W, P.H, cbase, zc, es, 1.0f / (float)P.N, nz, st);
 }
@@ -417,6 +596,20 @@ void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz,
     pass_c2c(P, W, W, P.H, 1, false, nz, st);
     FFTLen* f3 = get_fft(P.ffts, P.dims[2]);
     int n = f3->sh.n;
+    {
+        int nl = P.h1 * P.dims[1];
+        const NSItem* it = P.items.as<NSItem>();
+        int sy = analysis_masks ? 0 : 1;
+        switch (n) {
+            case 16: launch_accum_reg<16>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+            case 32: launch_accum_reg<32>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+            case 64: launch_accum_reg<64>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+            case 96: launch_accum_reg<96>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+            case 128: launch_accum_reg<128>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+            case 160: launch_accum_reg<160>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+            case 256: launch_accum_reg<256>(W, P.H, nz, P.tb, it, i0, sy, acc, comp, init, f3->sh.tw, nl, st); return;
+        }
+    }
     int T = pass_tile(n);
     while (T > 1 && T * n > kAccMax * 256) --T;
     if (T * n > kAccMax * 256) throw ArgError("axis 3 is too long for the accumulating pass of this build");
