@@ -81,6 +81,7 @@ SIGNATURES = {
     "sfl_stream_synthesize_next_index": (C.c_int, [P, C.POINTER(C.c_int32)]),
     "sfl_stream_synthesize_push": (C.c_int, [P, P, P]),
     "sfl_stream_synthesize_end": (C.c_int, [P, P, P]),
+    "sfl_ns_analyze_subband_static": (C.c_int, [P, P, P, C.c_int32, P]),
     "sfl_ns_design_table": (C.c_int, [C.POINTER(NSParams), Dims, C.c_char_p, C.c_int32,
                                       C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "sfl_surf_design_table": (C.c_int, [C.POINTER(SurfParams), Dims, C.c_char_p, C.c_int32,

@@ -480,6 +480,18 @@ int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream) {
     });
 }
 
+int sfl_ns_analyze_subband_static(sfl_plan* plan, const void* x, void* band, int32_t index, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(x, "x");
+        need(band, "band");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(band, plan->impl.dtype, "band");
+        on_device(plan, [&] { sfl::ns_analyze_subband_static(N, x, band, index, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
 int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const char* name, int32_t index,
                         double* out, int64_t* count) {
     return guarded([&] {

@@ -129,6 +129,8 @@ void ns_stream_synth_begin(NSPlan& P, cudaStream_t st);
 int ns_stream_synth_next_index(NSPlan& P, int* index);
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st);
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
+// One analysis subband with static scratch (noalloc.cu).
+void ns_analyze_subband_static(NSPlan& P, const void* x, void* band, int index, cudaStream_t st);
 
 // Decimated drivers (dec.cu)
 void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], int dtype);
