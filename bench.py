@@ -174,6 +174,7 @@ def main():
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip plain/secondary/cpu legs")
+    ap.add_argument("--group", type=int, default=0, help="subbands in flight per launch (0: the plan's default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))
@@ -194,6 +195,8 @@ def main():
     N = int(np.prod(DIMS))
     t = sfl.NSSurfacelet(**NS_KW)
     ws = sfl.make_workspace(t, "float32", DIMS)
+    if args.group > 0:
+        ws.set_group(args.group)
     S = ws.nsubbands
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     xs = [sfl.volume_like(DIMS).copy_(torch.randn(DIMS, device="cuda", generator=gen)) for _ in range(B)]

@@ -145,9 +145,22 @@ int sfl_plan_info(const sfl_plan* plan, int32_t* kind, int32_t dims[3], int32_t*
  * src/transforms/surfacelet.jl:444. */
 int sfl_subband_info(const sfl_plan* plan, int32_t i, int32_t shape[3], int64_t* offset);
 
+/* The plan's device status word, written by kernels whose bounded waits ran
+ * out (0 = fine, 1 = a bulk-copy barrier wait timed out).  Synchronizes with
+ * the device; reset != 0 clears it.  No counterpart in the reference. */
+int sfl_plan_status(sfl_plan* plan, int32_t* status, int32_t reset);
+
 /* Subbands a launch keeps in flight (NS: scratch holds that many spectra).
  * Default 8; only affects speed and scratch size. */
 int sfl_plan_set_group(sfl_plan* plan, int32_t group);
+
+/* NSSurfacelet kernel pipeline.  Both give the same subbands to float32
+ * rounding; they differ in speed only.  LINES (default): one line pass per
+ * axis.  PLANES: a pass along axis 1 plus a 2-D pass per axis-1 frequency
+ * plane (sizes 64, 96, 128 on axes 2 and 3 only).  Not during a stream. */
+#define SFL_PIPELINE_LINES 0
+#define SFL_PIPELINE_PLANES 1
+int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline);
 
 /* ── Transforms ─────────────────────────────────────────────────────────── */
 

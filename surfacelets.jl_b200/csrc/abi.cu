@@ -331,6 +331,24 @@ int sfl_subband_info(const sfl_plan* plan, int32_t i, int32_t shape[3], int64_t*
     });
 }
 
+int sfl_plan_status(sfl_plan* plan, int32_t* status, int32_t reset) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(status, "status");
+        *status = 0;
+        if (plan->impl.kind == SFL_KIND_NS && plan->impl.ns->status.p) {
+            on_device(plan, [&] {
+                int v = 0;
+                sfl::cuda_check(cudaMemcpy(&v, plan->impl.ns->status.p, sizeof(int), cudaMemcpyDeviceToHost),
+                                "cudaMemcpy(status)");
+                *status = v;
+                if (reset) sfl::cuda_check(cudaMemset(plan->impl.ns->status.p, 0, sizeof(int)), "cudaMemset(status)");
+            });
+        }
+        return SFL_OK;
+    });
+}
+
 int sfl_plan_set_group(sfl_plan* plan, int32_t group) {
     return guarded([&] {
         need(plan, "plan");
@@ -341,9 +359,28 @@ int sfl_plan_set_group(sfl_plan* plan, int32_t group) {
             on_device(plan, [&] {
                 cudaDeviceSynchronize();
                 N.work.alloc(sizeof(float2) * N.H * g);
+                N.acc.alloc(sizeof(float2) * N.H * std::max(N.nch, g * N.nch));
             });
             N.group = g;
         }
+        return SFL_OK;
+    });
+}
+
+int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline) {
+    return guarded([&] {
+        need(plan, "plan");
+        if (plan->impl.kind != SFL_KIND_NS) throw sfl::ArgError("pipeline selection applies to NSSurfacelet plans");
+        sfl::NSPlan& N = *plan->impl.ns;
+        if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+        on_device(plan, [&] {
+            if (pipeline == SFL_PIPELINE_LINES)
+                N.plane = false;
+            else if (pipeline == SFL_PIPELINE_PLANES)
+                sfl::ns_use_planes(N);
+            else
+                throw sfl::ArgError("unknown pipeline " + std::to_string(pipeline));
+        });
         return SFL_OK;
     });
 }

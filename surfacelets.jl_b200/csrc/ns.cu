@@ -242,6 +242,39 @@ static std::vector<float> to_f32(const std::vector<double>& v) {
     return o;
 }
 
+// Builds the plane-major copies of the group tables and switches the plan to
+// the plane-major pipeline: (k1, k2, k3) -> k2 + n2 (k3 + n3 k1).
+void ns_use_planes(NSPlan& P) {
+    if (!ns_plane_supported(P.dims[0], P.dims[1], P.dims[2]))
+        throw ArgError("the plane-major pipeline does not support size " + std::to_string(P.dims[0]) + "x" +
+                       std::to_string(P.dims[1]) + "x" + std::to_string(P.dims[2]));
+    if (!P.Gp.p) {
+        const NSDesign& D = P.design;
+        const int J = P.p.scales;
+        const int h1 = P.h1, n2 = P.dims[1], n3 = P.dims[2];
+        auto permute = [&](const std::vector<double>& g, std::vector<float>& dst) {
+            size_t base = dst.size();
+            dst.resize(base + g.size());
+            for (int k3 = 0; k3 < n3; ++k3)
+                for (int k2 = 0; k2 < n2; ++k2)
+                    for (int k1 = 0; k1 < h1; ++k1)
+                        dst[base + k2 + (size_t)n2 * (k3 + (size_t)n3 * k1)] =
+                            (float)g[k1 + (size_t)h1 * (k2 + (size_t)n2 * k3)];
+        };
+        std::vector<float> Gp, Blp;
+        for (int j = 1; j <= J; ++j)
+            for (int i = 1; i <= 3; ++i) permute(ns_group_mask(D, J - j, i, true), Gp);
+        if (!P.p.tight)
+            for (int lv = 0; lv < J; ++lv) permute(ns_group_mask(D, lv, 1, false), Blp);
+        upload(P.Gp, Gp);
+        upload(P.Blp, Blp);
+        P.tbp = P.tb;
+        P.tbp.G = P.Gp.as<float>();
+        P.tbp.Bl = P.Blp.as<float>();
+    }
+    P.plane = true;
+}
+
 void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype) {
     for (int d = 0; d < 3; ++d)
         if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
@@ -348,9 +381,11 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     get_fft(P.ffts, dims[2]);
 
     P.X.alloc(sizeof(float2) * P.H * P.nch);
+    P.status.alloc(sizeof(int));
+    cuda_check(cudaMemset(P.status.p, 0, sizeof(int)), "cudaMemset(status)");
     P.group = std::min(8, P.S);
     P.work.alloc(sizeof(float2) * P.H * P.group);
-    P.acc.alloc(sizeof(float2) * P.H * P.nch);
+    P.acc.alloc(sizeof(float2) * P.H * std::max(P.nch, P.group * P.nch));
     P.comp.alloc(sizeof(float2) * P.H * P.nch);
 }
 
@@ -510,6 +545,7 @@ void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz,
 }  // namespace
 
 void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
+    if (P.plane) return ns_plane_analyze(P, x, c, st, synth_masks);
     const int es = P.nch;
     for (int ch = 0; ch < P.nch; ++ch) {
         float2* X = P.X.as<float2>();
@@ -523,6 +559,7 @@ void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_m
 }
 
 void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
+    if (P.plane) return ns_plane_synthesize(P, c, x, st, analysis_masks);
     const int es = P.nch;
     for (int ch = 0; ch < P.nch; ++ch) {
         float2* A = P.acc.as<float2>();
@@ -538,6 +575,12 @@ void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool anal
 // ── streaming ────────────────────────────────────────────────────────────────
 
 void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
+    if (P.plane) {
+        ns_plane_stream_analyze_begin(P, x, st);
+        P.stream_mode = 1;
+        P.stream_pos = 0;
+        return;
+    }
     for (int ch = 0; ch < P.nch; ++ch)
         rfft3(P, reinterpret_cast<const float*>(x) + ch, P.nch, P.X.as<float2>() + ch * P.H, st);
     P.stream_mode = 1;
@@ -551,6 +594,12 @@ int ns_stream_analyze_next(NSPlan& P, void* band, int* index, cudaStream_t st) {
         return SFL_DONE;
     }
     const NSItem& it = P.items_host[P.stream_pos];
+    if (P.plane) {
+        ns_plane_stream_analyze_one(P, P.stream_pos, band, st);
+        *index = it.s;
+        P.stream_pos += 1;
+        return SFL_OK;
+    }
     for (int ch = 0; ch < P.nch; ++ch)
         analyze_items(P, P.X.as<float2>() + ch * P.H, reinterpret_cast<float*>(band) + ch, ZMap{}, P.nch,
                       P.stream_pos, 1, false, st);
@@ -574,6 +623,11 @@ int ns_stream_synth_next_index(NSPlan& P, int* index) {
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
     if (P.stream_mode != 2) throw StateError("no streaming synthesis is open on this plan");
     if (P.stream_pos >= P.S) throw StateError("every subband has already been pushed");
+    if (P.plane) {
+        ns_plane_stream_synth_push(P, P.stream_pos, band, st);
+        P.stream_pos += 1;
+        return;
+    }
     for (int ch = 0; ch < P.nch; ++ch)
         synth_items(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1, false,
                     P.acc.as<float2>() + ch * P.H, P.comp.as<float2>() + ch * P.H, P.stream_pos == 0, st);
@@ -583,6 +637,11 @@ void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
     if (P.stream_mode != 2 || P.stream_pos != P.S)
         throw StateError("streaming synthesis ended before every subband was pushed");
+    if (P.plane) {
+        ns_plane_stream_synth_end(P, x, st);
+        P.stream_mode = 0;
+        return;
+    }
     for (int ch = 0; ch < P.nch; ++ch)
         irfft3(P, P.acc.as<float2>() + ch * P.H, reinterpret_cast<float*>(x) + ch, P.nch, st);
     P.stream_mode = 0;

@@ -92,6 +92,11 @@ struct NSPlan {
     DevMem items;
     DevMem G, Bl, vec, planes;
     NSMaskTables tb;
+    // plane-major pipeline (sizes with pencil and plane kernels)
+    bool plane = false;
+    DevMem Gp, Blp;         // G and Bl in plane-major order
+    NSMaskTables tbp;
+    DevMem status;          // device status word of bounded waits (0 = fine)
     std::map<int, std::unique_ptr<FFTLen>> ffts;
     DevMem X;        // nch spectra
     DevMem work;     // group spectra
@@ -129,6 +134,15 @@ void ns_stream_synth_begin(NSPlan& P, cudaStream_t st);
 int ns_stream_synth_next_index(NSPlan& P, int* index);
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st);
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
+// Plane-major pipeline (ns_plane.cu).
+bool ns_plane_supported(int n1, int n2, int n3);
+void ns_use_planes(NSPlan& P);
+void ns_plane_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
+void ns_plane_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
+void ns_plane_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);
+void ns_plane_stream_analyze_one(NSPlan& P, int pos, void* band, cudaStream_t st);
+void ns_plane_stream_synth_push(NSPlan& P, int pos, const void* band, cudaStream_t st);
+void ns_plane_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
 // One analysis subband with static scratch (noalloc.cu).
 void ns_analyze_subband_static(NSPlan& P, const void* x, void* band, int index, cudaStream_t st);
 

@@ -335,6 +335,14 @@ class Workspace:
     def set_group(self, group):
         check(lib.sfl_plan_set_group(self._h, int(group)))
 
+    PIPELINES = {"lines": 0, "planes": 1}
+
+    def set_pipeline(self, name):
+        """NSSurfacelet kernel pipeline: "lines" (default) or "planes"."""
+        if name not in self.PIPELINES:
+            raise ArgumentError(f"unknown pipeline {name!r}; expected one of {sorted(self.PIPELINES)}")
+        check(lib.sfl_plan_set_pipeline(self._h, self.PIPELINES[name]))
+
     def subband_info(self, i):
         """(shape, element offset) of subband i (1-based)."""
         return self._info[i - 1]

@@ -34,16 +34,22 @@ CASES = [
     ((32, 32, 32), dict(scales=3, direction_levels=[2, 2, 3])),
     ((26, 30, 12), dict(scales=1, direction_levels=[3], bernstein_order=6, transition=0.5)),
     ((16, 12, 20), dict(scales=2, direction_levels=[1, 2], bernstein_order=6, tight=False)),
+    # sizes the plane-major pipeline also supports
+    ((64, 64, 64), dict(scales=3, direction_levels=[2, 2, 3])),
+    ((96, 64, 128), dict(scales=2, direction_levels=[1, 3], bernstein_order=6)),
+    ((128, 128, 64), dict(scales=2, direction_levels=[2, 2], bernstein_order=8, tight=False)),
 ]
+PIPELINE_CASES = [(d, k, "lines") for d, k in CASES] + [(d, k, "planes") for d, k in CASES[-3:]]
 
 
-@pytest.mark.parametrize("dims,kw", CASES)
-def test_analyze_synthesize_match_oracle(sfl, dims, kw):
+@pytest.mark.parametrize("dims,kw,pipeline", PIPELINE_CASES)
+def test_analyze_synthesize_match_oracle(sfl, dims, kw, pipeline):
     rng = np.random.default_rng(202)
     x = rng.standard_normal(dims).astype(np.float32)
     t = sfl.NSSurfacelet(**kw)
     T = oracle_tables(dims, **kw)
     ws = sfl.make_workspace(t, "float32", dims)
+    ws.set_pipeline(pipeline)
     xd = sfl.to_device(x)
     c = sfl.analyze(t, xd, workspace=ws)
     ch = sfl.to_host(c)
@@ -57,6 +63,10 @@ def test_analyze_synthesize_match_oracle(sfl, dims, kw):
     cr = rng.standard_normal(cref.shape).astype(np.float32)
     y = sfl.to_host(sfl.synthesize(t, sfl.to_device(cr), workspace=ws))
     assert rel_l2(y, N.synthesize(T, cr.astype(np.float64))) <= REL
+    # no bounded wait of the kernels ran out
+    import ctypes as C
+    st = C.c_int32(-1)
+    assert sfl.lib.sfl_plan_status(ws._h, C.byref(st), 0) == 0 and st.value == 0
 
 
 @pytest.mark.parametrize("dims,kw", [CASES[0], CASES[2], CASES[6]])
@@ -130,6 +140,31 @@ def test_streaming_matches_materialized(sfl):
         sfl.synthesize_(lambda i: sfl.volume_like((4, 4, 4)), sfl.volume_like(dims), ws)
 
 
+@pytest.mark.parametrize("dims,pipeline", [((64, 64, 64), "lines"), ((64, 64, 64), "planes"),
+                                           ((16, 16, 16), "lines")])
+@pytest.mark.parametrize("dtype", ["float32", "complex64"])
+def test_streaming_equals_materialized_bit_for_bit(sfl, dims, pipeline, dtype):
+    # test/items/test_ns_surfacelet.jl:79-106, 108-138
+    import torch
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[1, 2], bernstein_order=6)
+    rng = np.random.default_rng(96)
+    x = rng.standard_normal(dims).astype(np.float32)
+    if dtype == "complex64":
+        x = (x + 1j * rng.standard_normal(dims)).astype(np.complex64)
+    ws = sfl.make_workspace(t, dtype, dims)
+    ws.set_pipeline(pipeline)
+    xd = sfl.to_device(x)
+    ref = sfl.analyze(ws, xd)
+    got = {}
+    sfl.analyze(lambda i, b: got.__setitem__(i, b.clone()), ws, xd)
+    for i in range(1, ws.nsubbands + 1):
+        assert torch.equal(got[i], ref[..., i - 1]), i
+    y = sfl.volume_like(dims, dtype)
+    sfl.synthesize_(lambda i: ref[..., i - 1], y, ws)
+    assert torch.equal(y, sfl.synthesize(ws, ref))
+    assert rel_l2(sfl.to_host(y), x) <= REL
+
+
 def test_group_size_does_not_change_results(sfl):
     dims = (20, 16, 12)
     t = sfl.NSSurfacelet(scales=2, direction_levels=[2, 3], bernstein_order=6)
@@ -139,6 +174,15 @@ def test_group_size_does_not_change_results(sfl):
     ca, cb = sfl.analyze(a, x), sfl.analyze(b, x)
     assert bool((ca == cb).all())
     assert bool((sfl.synthesize(a, ca) == sfl.synthesize(b, ca)).all())
+
+
+def test_pipeline_selection_is_validated(sfl):
+    ws = sfl.make_workspace(sfl.NSSurfacelet(scales=1, direction_levels=[1], bernstein_order=4), "float32", (12, 10, 8))
+    with pytest.raises(sfl.ArgumentError, match="plane-major pipeline does not support"):
+        ws.set_pipeline("planes")
+    with pytest.raises(sfl.ArgumentError, match="unknown pipeline"):
+        ws.set_pipeline("slabs?")
+    ws.set_pipeline("lines")
 
 
 def test_workspace_validation(sfl):
