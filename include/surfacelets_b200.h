@@ -154,12 +154,18 @@ int sfl_plan_status(sfl_plan* plan, int32_t* status, int32_t reset);
  * Default 8; only affects speed and scratch size. */
 int sfl_plan_set_group(sfl_plan* plan, int32_t group);
 
-/* NSSurfacelet kernel pipeline.  Both give the same subbands to float32
- * rounding; they differ in speed only.  LINES (default): one line pass per
- * axis.  PLANES: a pass along axis 1 plus a 2-D pass per axis-1 frequency
- * plane (sizes 64, 96, 128 on axes 2 and 3 only).  Not during a stream. */
+/* NSSurfacelet kernel pipeline.  All give the same subbands to float32
+ * rounding; they differ in speed only.
+ *   SLABS (default where supported: axes 1 and 2 of length 64, 96, 128 or
+ *     160): a line pass along axis 3 plus one pass per axis-3 slab, skipping
+ *     the zero rows and columns of band-limited masks.
+ *   LINES (default elsewhere): one line pass per axis.
+ *   PLANES: a pass along axis 1 plus a 2-D pass per axis-1 frequency plane
+ *     (axes 2 and 3 of length 64, 96 or 128).
+ * Not while a streaming pass is open. */
 #define SFL_PIPELINE_LINES 0
 #define SFL_PIPELINE_PLANES 1
+#define SFL_PIPELINE_SLABS 2
 int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline);
 
 /* ── Transforms ─────────────────────────────────────────────────────────── */

@@ -355,13 +355,13 @@ int sfl_plan_set_group(sfl_plan* plan, int32_t group) {
         if (group < 1) throw sfl::ArgError("group must be ≥ 1, got " + std::to_string(group));
         if (plan->impl.kind == SFL_KIND_NS) {
             sfl::NSPlan& N = *plan->impl.ns;
+            if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
             int g = std::min<int>(group, N.S);
             on_device(plan, [&] {
                 cudaDeviceSynchronize();
-                N.work.alloc(sizeof(float2) * N.H * g);
-                N.acc.alloc(sizeof(float2) * N.H * std::max(N.nch, g * N.nch));
+                N.group = g;
+                sfl::ns_alloc_scratch(N);
             });
-            N.group = g;
         }
         return SFL_OK;
     });
@@ -374,10 +374,18 @@ int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline) {
         sfl::NSPlan& N = *plan->impl.ns;
         if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
         on_device(plan, [&] {
-            if (pipeline == SFL_PIPELINE_LINES)
+            cudaDeviceSynchronize();
+            if (pipeline == SFL_PIPELINE_LINES) {
                 N.plane = false;
-            else if (pipeline == SFL_PIPELINE_PLANES)
+                if (N.slab) {
+                    N.slab = false;
+                    sfl::ns_alloc_scratch(N);
+                }
+            } else if (pipeline == SFL_PIPELINE_PLANES) {
                 sfl::ns_use_planes(N);
+            } else if (pipeline == SFL_PIPELINE_SLABS) {
+                sfl::ns_use_slabs(N);
+            }
             else
                 throw sfl::ArgError("unknown pipeline " + std::to_string(pipeline));
         });

@@ -273,6 +273,10 @@ void ns_use_planes(NSPlan& P) {
         P.tbp.Bl = P.Blp.as<float>();
     }
     P.plane = true;
+    if (P.slab) {
+        P.slab = false;
+        ns_alloc_scratch(P);
+    }
 }
 
 void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype) {
@@ -294,10 +298,12 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     {
         std::vector<float> G;
         G.reserve((size_t)3 * J * P.H);
+        P.boxes.clear();
         for (int j = 1; j <= J; ++j)
             for (int i = 1; i <= 3; ++i) {
                 std::vector<double> g = ns_group_mask(D, J - j, i, true);
                 for (double v : g) G.push_back((float)v);
+                P.boxes.push_back(ns_table_box(g, P.h1, dims[1], dims[2]));
             }
         upload(P.G, G);
         std::vector<float> Bl;
@@ -305,8 +311,23 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
             for (int lv = 0; lv < J; ++lv) {
                 std::vector<double> b = ns_group_mask(D, lv, 1, false);
                 for (double v : b) Bl.push_back((float)v);
+                // the synthesis bandpass B_j covers the group factors of its level
+                const NSBox bb = ns_table_box(b, P.h1, dims[1], dims[2]);
+                for (int i = 0; i < 3; ++i) P.boxes[3 * (J - 1 - lv) + i] = bb;
             }
         upload(P.Bl, Bl);
+    }
+    {
+        // lowpass box from its per-axis factors
+        int m1 = -1, m2 = -1;
+        const auto& a1 = D.pa[J][0];
+        const auto& a2 = D.pa[J][1];
+        for (int k = 0; k < (int)a1.size(); ++k)
+            if (a1[k] != 0.0) m1 = std::max(m1, k);
+        for (int k = 0; k < (int)a2.size(); ++k)
+            if (a2[k] != 0.0) m2 = std::max(m2, std::min(k, dims[1] - k));
+        P.boxes.push_back(ns_make_box(m1 + 1, m2, dims[1]));
+        P.boxes_full = ns_make_box(P.h1, dims[1], dims[1]);
     }
     std::vector<float> vec;
     for (int d = 0; d < 3; ++d) {
@@ -380,13 +401,31 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     get_fft(P.ffts, dims[1]);
     get_fft(P.ffts, dims[2]);
 
-    P.X.alloc(sizeof(float2) * P.H * P.nch);
     P.status.alloc(sizeof(int));
     cuda_check(cudaMemset(P.status.p, 0, sizeof(int)), "cudaMemset(status)");
     P.group = std::min(8, P.S);
-    P.work.alloc(sizeof(float2) * P.H * P.group);
-    P.acc.alloc(sizeof(float2) * P.H * std::max(P.nch, P.group * P.nch));
-    P.comp.alloc(sizeof(float2) * P.H * P.nch);
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&P.sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    P.P1 = P.h1;
+    while (P.P1 % 4 != 2) ++P.P1;
+    P.SP = (long long)P.P1 * dims[1] * dims[2];
+    P.slab = ns_slab_supported(dims[0], dims[1], dims[2]);
+    ns_alloc_scratch(P);
+}
+
+// Spectrum-sized scratch for the selected pipeline and group size.
+void ns_alloc_scratch(NSPlan& P) {
+    const long long spec = P.slab ? P.SP : P.H;
+    P.X.alloc(sizeof(float2) * spec * P.nch);
+    P.work.alloc(sizeof(float2) * spec * P.group);
+    if (P.slab) {
+        P.acc.alloc(sizeof(float2) * spec * P.nch);
+        P.comp.alloc(0);
+    } else {
+        P.acc.alloc(sizeof(float2) * P.H * std::max(P.nch, P.group * P.nch));
+        P.comp.alloc(sizeof(float2) * P.H * P.nch);
+    }
 }
 
 // ── passes ───────────────────────────────────────────────────────────────────
@@ -545,6 +584,7 @@ void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz,
 }  // namespace
 
 void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
+    if (P.slab) return ns_slab_analyze(P, x, c, st, synth_masks);
     if (P.plane) return ns_plane_analyze(P, x, c, st, synth_masks);
     const int es = P.nch;
     for (int ch = 0; ch < P.nch; ++ch) {
@@ -559,6 +599,7 @@ void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_m
 }
 
 void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
+    if (P.slab) return ns_slab_synthesize(P, c, x, st, analysis_masks);
     if (P.plane) return ns_plane_synthesize(P, c, x, st, analysis_masks);
     const int es = P.nch;
     for (int ch = 0; ch < P.nch; ++ch) {
@@ -575,6 +616,12 @@ void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool anal
 // ── streaming ────────────────────────────────────────────────────────────────
 
 void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
+    if (P.slab) {
+        ns_slab_stream_analyze_begin(P, x, st);
+        P.stream_mode = 1;
+        P.stream_pos = 0;
+        return;
+    }
     if (P.plane) {
         ns_plane_stream_analyze_begin(P, x, st);
         P.stream_mode = 1;
@@ -594,6 +641,12 @@ int ns_stream_analyze_next(NSPlan& P, void* band, int* index, cudaStream_t st) {
         return SFL_DONE;
     }
     const NSItem& it = P.items_host[P.stream_pos];
+    if (P.slab) {
+        ns_slab_stream_analyze_one(P, P.stream_pos, band, st);
+        *index = it.s;
+        P.stream_pos += 1;
+        return SFL_OK;
+    }
     if (P.plane) {
         ns_plane_stream_analyze_one(P, P.stream_pos, band, st);
         *index = it.s;
@@ -623,6 +676,11 @@ int ns_stream_synth_next_index(NSPlan& P, int* index) {
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
     if (P.stream_mode != 2) throw StateError("no streaming synthesis is open on this plan");
     if (P.stream_pos >= P.S) throw StateError("every subband has already been pushed");
+    if (P.slab) {
+        ns_slab_stream_synth_push(P, P.stream_pos, band, st);
+        P.stream_pos += 1;
+        return;
+    }
     if (P.plane) {
         ns_plane_stream_synth_push(P, P.stream_pos, band, st);
         P.stream_pos += 1;
@@ -637,6 +695,11 @@ void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
     if (P.stream_mode != 2 || P.stream_pos != P.S)
         throw StateError("streaming synthesis ended before every subband was pushed");
+    if (P.slab) {
+        ns_slab_stream_synth_end(P, x, st);
+        P.stream_mode = 0;
+        return;
+    }
     if (P.plane) {
         ns_plane_stream_synth_end(P, x, st);
         P.stream_mode = 0;

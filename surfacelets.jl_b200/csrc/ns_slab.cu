@@ -1,0 +1,777 @@
+// NSSurfacelet slab pipeline for sm_100a: per subband one line pass along
+// axis 3 and one pass over the axis-3 slabs, with the zero rows and columns of
+// band-limited masks skipped.
+//
+// Spectra (the input spectrum X, the per-subband intermediates Y and the
+// synthesis accumulator) live on the rfft grid (h1, n2, n3) with the axis-1
+// pitch padded to P1 (P1 >= h1, P1 = 2 mod 4): bin (k1, k2, k3) sits at
+// k1 + P1 (k2 + n2 k3), so one slab (fixed k3 or n3) is a contiguous block of
+// P1 n2 bins that a CTA holds in shared memory.
+//
+//   analysis of subband s, c_s = irfft(X M_s):
+//     line pass  Y_s(k1, k2, n3) = IFFT_3(X M_s)(k1, k2, .) for the lines of
+//                the mask's support box (mask applied on load);
+//     slab pass  per n3: IFFT_2 of the rows k1 < nk1, then the C2R along
+//                axis 1 of two columns at a time, written straight into c_s.
+//   synthesis, x = irfft(sum_s M_s rfft(c_s)):
+//     slab pass  per n3: R2C along axis 1 (two columns at a time), FFT_2 of
+//                the rows in the box -> Y_s;
+//     line pass  FFT_3 of Y_s times M_s, summed over the subbands of one mask
+//                group in registers, one accumulator round trip per group;
+//     then the irfft of the accumulator (line pass and slab pass, no mask).
+//
+// Support boxes: the group factor B_j of scale j is a product of per-axis
+// raised-cosine lowpass profiles of the finer levels
+// (src/pyramid/fourier_pyramid.jl:143-150, src/transforms/ns_surfacelet.jl:
+// 271-272), so it vanishes outside |k_d| <= b_d.  The plan scans each
+// float64-designed group table for its box; lines and rows outside it are
+// neither loaded nor transformed, and read as zeros downstream.
+//
+// Inside the slab pass the N2 lanes of a line sit in one warp, and the
+// exchange between the two in-register DFT steps goes through the line's own
+// slots of the slab (a row, or the two columns of a pair) with an XOR
+// swizzle, so it needs only __syncwarp; CTA-wide barriers separate the
+// phases.
+#include <algorithm>
+#include <cstring>
+
+#include "ns_mask.cuh"
+#include "plan.h"
+#include "prof.h"
+#include "regpass.cuh"
+
+namespace sfl {
+
+namespace {
+
+constexpr int kSlabThreads = 512;
+constexpr int kSlabWarps = kSlabThreads / 32;
+constexpr size_t kSlabSmemMax = 112 * 1024;   // two CTAs an SM
+
+// ── lines along axis 3 of a padded spectrum, restricted to a box ───────────
+
+// Line l = (k1, j) with k1 fastest; column j maps to k2 = j for j <= b2 and
+// to the negative frequencies n2 - (nk2 - j) above.
+struct BoxMap {
+    int nk1, nk2, b2, n2;
+    __device__ __forceinline__ void k12(int l, int& k1, int& k2) const {
+        const int j = l / nk1;
+        k1 = l - j * nk1;
+        k2 = j <= b2 ? j : j + (n2 - nk2);
+    }
+};
+
+struct L3LoadC {
+    const float2* src;
+    long long zstride;
+    int P1, s3;
+    BoxMap bx;
+    struct Ctx {
+        const float2* p;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const {
+        int k1 = 0, k2 = 0;
+        if (valid) bx.k12(l, k1, k2);
+        return Ctx{src + z * zstride + k1 + P1 * k2};
+    }
+    __device__ __forceinline__ float2 get(const Ctx& c, int i) const { return c.p[i * s3]; }
+};
+
+struct L3StoreC {
+    static constexpr bool kStaged = false;
+    float2* dst;
+    long long zstride;
+    int P1, s3;
+    BoxMap bx;
+    struct Ctx {
+        float2* p;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const {
+        int k1 = 0, k2 = 0;
+        if (valid) bx.k12(l, k1, k2);
+        return Ctx{dst + z * zstride + k1 + P1 * k2};
+    }
+    __device__ __forceinline__ void put(const Ctx& c, int k, float2 v) const { c.p[k * s3] = v; }
+};
+
+// X times the analysis (or synthesis) mask of item z, on load.
+struct L3LoadMask {
+    const float2* X;
+    int P1, s3;
+    BoxMap bx;
+    NSMaskTables tb;
+    const NSItem* items;
+    int item0;
+    int synth;
+    struct Ctx {
+        const float2* x;
+        NSMaskLine m;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const {
+        int k1 = 0, k2 = 0;
+        if (valid) bx.k12(l, k1, k2);
+        Ctx c;
+        c.x = X + k1 + P1 * k2;
+        c.m = ns_mask_line(tb, items[item0 + z], k1 + tb.h1 * k2, synth != 0);
+        return c;
+    }
+    __device__ __forceinline__ float2 get(const Ctx& c, int i) const {
+        return c_scale(c.x[i * s3], ns_mask_at(c.m, i, (long long)tb.h1 * tb.n2));
+    }
+};
+
+// Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
+// summed in registers into the accumulator (plain float32 sums, item order).
+template <int N>
+__global__ void __launch_bounds__(256, 2) ns_slab_accum_kernel(const float2* __restrict__ Y, long long ystride, int G,
+                                                            int P1, int s3, BoxMap bx, NSMaskTables tb,
+                                                            const NSItem* __restrict__ items, int item0, int synth,
+                                                            float2* acc, const float2* __restrict__ tw, int nlines) {
+    using Ge = RegGeom<N>;
+    constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
+    extern __shared__ float2 xch[];
+    const int tid = threadIdx.x;
+    const int lp = tid % LP, p = tid / LP;
+    const int l = blockIdx.x * LP + lp;
+    const bool valid = l < nlines;
+    int k1 = 0, k2 = 0;
+    if (valid) bx.k12(l, k1, k2);
+    float2* a = acc + k1 + P1 * k2;
+    float2* xl = xch + lp * Ge::XLINE;
+    float2 s[E];
+#pragma unroll
+    for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+        for (int k = 0; k < N2; ++k)
+            s[j * N2 + k] = valid ? a[((p + N2 * j) + N1 * k) * s3] : make_float2(0.f, 0.f);
+    const long long si_nat = (long long)tb.h1 * tb.n2;
+    for (int z = 0; z < G; ++z) {
+        L3LoadC ld{Y + z * ystride, 0, P1, s3, bx};
+        L3LoadC::Ctx lc{ld.src + k1 + P1 * k2};
+        float2 u[E];
+        reg_line_fft<N, false>(ld, lc, valid, p, xl, tw, u);
+        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], k1 + tb.h1 * k2, synth != 0);
+#pragma unroll
+        for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+            for (int k = 0; k < N2; ++k) {
+                const int k3 = (p + N2 * j) + N1 * k;
+                s[j * N2 + k] = c_add(s[j * N2 + k], c_scale(u[j * N2 + k], ns_mask_at(mk, k3, si_nat)));
+            }
+        __syncthreads();   // the exchange rows are reused by the next item
+    }
+    if (valid) {
+#pragma unroll
+        for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+            for (int k = 0; k < N2; ++k) a[((p + N2 * j) + N1 * k) * s3] = s[j * N2 + k];
+    }
+}
+
+// ── slab passes ─────────────────────────────────────────────────────────────
+
+struct SlabArgs {
+    float2* spec;            // padded spectra, item z at spec + z * spec_zstride
+    long long spec_zstride;
+    float* vol;              // real volumes (element stride es), item z at vol + vz.off(z)
+    ZMap vz;
+    int es;
+    float scale;             // applied to the C2R outputs
+    int P1, n3;
+    int nk1, nk2, b2;        // box: rows k1 < nk1, columns as BoxMap
+    int units;               // items x n3
+    const float2* twa;       // w_n1^k, k < n1 (float64-designed)
+    const float2* twb;       // w_n2^k, k < n2
+};
+
+template <int N>
+struct SlabLine {
+    static constexpr int N1 = LinePlan<N>::N1;
+    static constexpr int N2 = LinePlan<N>::N2;
+    static constexpr int M = N1 / N2;
+    static constexpr int LPW = 32 / N2;             // lines a warp
+    static constexpr int LPR = kSlabWarps * LPW;    // lines a round
+};
+
+// Twiddles of a line FFT rearranged as tw2[m * N2 + p] = w_N^{p m}: the N2
+// lanes of a line read consecutive words.
+template <int N>
+__device__ __forceinline__ void load_slab_twiddles(float2* tw2, const float2* __restrict__ tw) {
+    using L = SlabLine<N>;
+    for (int i = threadIdx.x; i < L::N1 * L::N2; i += blockDim.x) {
+        const int m = i / L::N2, p = i - m * L::N2;
+        tw2[i] = tw[p * m];
+    }
+}
+
+// FFT of one line of N points held by the N2 lanes p of a warp: v[r] holds
+// x[p + N2 r] on entry and X[(p + N2 j) + N1 k] at v[j N2 + k] on exit.  The
+// exchange runs through slot(t), t < N, which only this line touches; lanes
+// of invalid lines skip every slot access but keep to the warp barriers.
+template <int N, bool INV, class Slot>
+__device__ __forceinline__ void warp_line_fft(float2 (&v)[LinePlan<N>::N1], int p, bool valid,
+                                              const float2* __restrict__ tw2, const Slot& slot) {
+    using L = SlabLine<N>;
+    constexpr int N1 = L::N1, N2 = L::N2;
+    RegDft<N1, INV>::run(v);
+#pragma unroll
+    for (int m = 1; m < N1; ++m) {
+        float2 w = tw2[m * N2 + p];
+        if (INV) w.y = -w.y;
+        v[m] = c_mul(v[m], w);
+    }
+    __syncwarp();   // the line's inputs may have come from its own slots
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < N1; ++m) *slot(m * N2 + (p ^ (m & (N2 - 1)))) = v[m];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < L::M; ++j) {
+        const int m = p + N2 * j;
+        float2 w[N2];
+#pragma unroll
+        for (int pp = 0; pp < N2; ++pp) w[pp] = valid ? *slot(m * N2 + (pp ^ p)) : make_float2(0.f, 0.f);
+        RegDft<N2, INV>::run(w);
+#pragma unroll
+        for (int k = 0; k < N2; ++k) v[j * N2 + k] = w[k];
+    }
+    __syncwarp();   // slots are free again
+}
+
+// Lane layout of the column-pair phases: p fastest, then the line; with four
+// lines a warp, the two lines of a half warp are two apart so that their
+// columns fall on disjoint banks (P1 = 2 mod 4).
+template <int N>
+__device__ __forceinline__ int pair_subline(int s) {
+    if (SlabLine<N>::LPW == 4) return s == 1 ? 2 : (s == 2 ? 1 : s);
+    return s;
+}
+
+struct RowSlot {
+    float2* base;
+    int P1;
+    __device__ __forceinline__ float2* operator()(int t) const { return base + P1 * t; }
+};
+
+struct PairSlot {
+    float2* a;
+    float2* b;
+    int split;
+    __device__ __forceinline__ float2* operator()(int t) const { return t < split ? a + t : b + (t - split); }
+};
+
+template <int NA, int NB>
+struct SlabSmem {
+    static size_t bytes(int P1) { return sizeof(float2) * ((size_t)NA + NB + (size_t)P1 * NB); }
+};
+
+// Analysis slab pass (inverse): spectra -> real volumes.
+template <int NA, int NB, int MINB>
+__global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArgs a) {
+    using LA = SlabLine<NA>;
+    using LB = SlabLine<NB>;
+    extern __shared__ float2 sm[];
+    float2* twA = sm;
+    float2* twB = sm + NA;
+    float2* S = sm + NA + NB;
+    load_slab_twiddles<NA>(twA, a.twa);
+    load_slab_twiddles<NB>(twB, a.twb);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int P1 = a.P1;
+    const int SL = P1 * NB;
+    const long long plane = (long long)NA * NB;
+    for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
+        const int z = u / a.n3, s3 = u - z * a.n3;
+        const float2* src = a.spec + z * a.spec_zstride + (long long)s3 * SL;
+        // 1. the box of the slab into shared memory
+        for (int j = warp; j < a.nk2; j += kSlabWarps) {
+            const int k2 = j <= a.b2 ? j : j + (NB - a.nk2);
+            for (int k1 = lane; k1 < a.nk1; k1 += 32) S[k1 + P1 * k2] = src[k1 + P1 * k2];
+        }
+        __syncthreads();
+        // 2. inverse FFT along axis 2 of the rows k1 < nk1; columns outside the box are zero
+        {
+            const int p = lane % LB::N2, s = lane / LB::N2;
+            for (int base = 0; base < a.nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= a.nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < a.nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) {
+                    const int k2 = p + LB::N2 * r;
+                    const bool in = valid && (k2 <= a.b2 || k2 >= NB - (a.nk2 - a.b2 - 1));
+                    v[r] = in ? row[P1 * k2] : make_float2(0.f, 0.f);
+                }
+                warp_line_fft<NB, true>(v, p, valid, twB, RowSlot{row, P1});
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
+        __syncthreads();
+        // 3. C2R along axis 1, columns 2l and 2l+1 as one complex line; rows k1 >= nk1 are zero
+        {
+            const int p = lane % LA::N2, s = pair_subline<NA>(lane / LA::N2);
+            constexpr int npairs = NB / 2;
+            float* out = a.vol + a.vz.off(z) + (long long)s3 * plane * a.es;
+            for (int base = 0; base < npairs; base += LA::LPR) {
+                if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
+                const int l = base + warp * LA::LPW + s;
+                const bool valid = l < npairs;
+                float2* ca = S + P1 * (2 * (valid ? l : 0));
+                float2* cb = ca + P1;
+                float2 v[LA::N1];
+#pragma unroll
+                for (int r = 0; r < LA::N1; ++r) {
+                    const int i = p + LA::N2 * r;
+                    const int k = 2 * i <= NA ? i : NA - i;
+                    float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+                    if (valid && k < a.nk1) {
+                        A = ca[k];
+                        B = cb[k];
+                    }
+                    if (k == 0 || 2 * k == NA) {
+                        A.y = 0.f;
+                        B.y = 0.f;
+                    }
+                    v[r] = 2 * i <= NA ? make_float2(A.x - B.y, A.y + B.x) : make_float2(A.x + B.y, B.x - A.y);
+                }
+                warp_line_fft<NA, true>(v, p, valid, twA, PairSlot{ca, cb, (NA + 1) / 2});
+                if (valid) {
+                    float* oa = out + (long long)(2 * l) * NA * a.es;
+                    float* ob = oa + (long long)NA * a.es;
+#pragma unroll
+                    for (int j = 0; j < LA::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LA::N2; ++k) {
+                            const int i1 = (p + LA::N2 * j) + LA::N1 * k;
+                            oa[i1 * a.es] = v[j * LA::N2 + k].x * a.scale;
+                            ob[i1 * a.es] = v[j * LA::N2 + k].y * a.scale;
+                        }
+                }
+            }
+        }
+        __syncthreads();   // the slab buffer is reused by the next unit
+    }
+}
+
+// Synthesis / rfft slab pass (forward): real volumes -> spectra (the box rows).
+template <int NA, int NB, int MINB>
+__global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArgs a) {
+    using LA = SlabLine<NA>;
+    using LB = SlabLine<NB>;
+    constexpr int H1 = NA / 2 + 1;
+    constexpr int QA = (H1 + LA::N2 - 1) / LA::N2;   // output bins a lane unpacks
+    extern __shared__ float2 sm[];
+    float2* twA = sm;
+    float2* twB = sm + NA;
+    float2* S = sm + NA + NB;
+    load_slab_twiddles<NA>(twA, a.twa);
+    load_slab_twiddles<NB>(twB, a.twb);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int P1 = a.P1;
+    const int SL = P1 * NB;
+    const long long plane = (long long)NA * NB;
+    for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
+        const int z = u / a.n3, s3 = u - z * a.n3;
+        // 1. R2C along axis 1 of columns 2l, 2l+1 (as the real and imaginary parts of one line)
+        {
+            const int p = lane % LA::N2, s = pair_subline<NA>(lane / LA::N2);
+            constexpr int npairs = NB / 2;
+            const float* in = a.vol + a.vz.off(z) + (long long)s3 * plane * a.es;
+            for (int base = 0; base < npairs; base += LA::LPR) {
+                if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
+                const int l = base + warp * LA::LPW + s;
+                const bool valid = l < npairs;
+                const float* ia = in + (long long)(2 * (valid ? l : 0)) * NA * a.es;
+                const float* ib = ia + (long long)NA * a.es;
+                float2 v[LA::N1];
+#pragma unroll
+                for (int r = 0; r < LA::N1; ++r) {
+                    const int i = p + LA::N2 * r;
+                    v[r] = valid ? make_float2(ia[i * a.es], ib[i * a.es]) : make_float2(0.f, 0.f);
+                }
+                float2* ca = S + P1 * (2 * (valid ? l : 0));
+                float2* cb = ca + P1;
+                const PairSlot slot{ca, cb, (NA + 1) / 2};
+                warp_line_fft<NA, false>(v, p, valid, twA, slot);
+                // Z in natural order through the pair's slots, then the two half spectra
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LA::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LA::N2; ++k) *slot((p + LA::N2 * j) + LA::N1 * k) = v[j * LA::N2 + k];
+                }
+                __syncwarp();
+                float2 ha[QA], hb[QA];
+#pragma unroll
+                for (int q = 0; q < QA; ++q) {
+                    const int k = p + LA::N2 * q;
+                    ha[q] = hb[q] = make_float2(0.f, 0.f);
+                    if (valid && k < a.nk1) {
+                        const float2 zk = *slot(k);
+                        const float2 zn = *slot(k == 0 ? 0 : NA - k);
+                        ha[q] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+                        hb[q] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+                    }
+                }
+                __syncwarp();
+                if (valid) {
+#pragma unroll
+                    for (int q = 0; q < QA; ++q) {
+                        const int k = p + LA::N2 * q;
+                        if (k < a.nk1) {
+                            ca[k] = ha[q];
+                            cb[k] = hb[q];
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // 2. forward FFT along axis 2 of the rows k1 < nk1
+        {
+            const int p = lane % LB::N2, s = lane / LB::N2;
+            for (int base = 0; base < a.nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= a.nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < a.nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) v[r] = valid ? row[P1 * (p + LB::N2 * r)] : make_float2(0.f, 0.f);
+                warp_line_fft<NB, false>(v, p, valid, twB, RowSlot{row, P1});
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
+        __syncthreads();
+        // 3. the box of the slab out to the spectrum
+        float2* dst = a.spec + z * a.spec_zstride + (long long)s3 * SL;
+        for (int j = warp; j < a.nk2; j += kSlabWarps) {
+            const int k2 = j <= a.b2 ? j : j + (NB - a.nk2);
+            for (int k1 = lane; k1 < a.nk1; k1 += 32) dst[k1 + P1 * k2] = S[k1 + P1 * k2];
+        }
+        __syncthreads();   // the slab buffer is reused by the next unit
+    }
+}
+
+// ── launch tables ────────────────────────────────────────────────────────────
+
+template <int N>
+constexpr int slab_minb() {
+    return LinePlan<N>::N1 <= 16 ? 2 : 1;
+}
+
+// One CTA a unit up to the resident capacity; CTAs stride over the rest.
+template <bool INV, int NA, int NB>
+void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
+    constexpr int MINB = (slab_minb<NA>() == 2 && slab_minb<NB>() == 2) ? 2 : 1;
+    auto kern = INV ? ns_slab_inv_kernel<NA, NB, MINB> : ns_slab_fwd_kernel<NA, NB, MINB>;
+    static size_t configured = 0;
+    static int resident = 0;
+    if (configured < smem) {
+        cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                   "cudaFuncSetAttribute(slab)");
+        configured = smem;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kSlabThreads, smem),
+                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor(slab)");
+        resident = std::max(resident, 1);
+    }
+    const int grid = std::max(1, std::min(a.units, resident * sms));
+    int tok = prof_begin(tag, st);
+    kern<<<grid, kSlabThreads, smem, st>>>(a);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "slab kernel launch");
+}
+
+template <bool INV, int NA>
+bool launch_slab_n(int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
+    switch (nb) {
+        case 64: launch_slab_nn<INV, NA, 64>(a, sms, smem, st, tag); return true;
+        case 96: launch_slab_nn<INV, NA, 96>(a, sms, smem, st, tag); return true;
+        case 128: launch_slab_nn<INV, NA, 128>(a, sms, smem, st, tag); return true;
+        case 160: launch_slab_nn<INV, NA, 160>(a, sms, smem, st, tag); return true;
+    }
+    return false;
+}
+
+template <bool INV>
+void launch_slab(int na, int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
+    bool ok = false;
+    switch (na) {
+        case 64: ok = launch_slab_n<INV, 64>(nb, a, sms, smem, st, tag); break;
+        case 96: ok = launch_slab_n<INV, 96>(nb, a, sms, smem, st, tag); break;
+        case 128: ok = launch_slab_n<INV, 128>(nb, a, sms, smem, st, tag); break;
+        case 160: ok = launch_slab_n<INV, 160>(nb, a, sms, smem, st, tag); break;
+    }
+    if (!ok) throw ArgError("no slab kernel for this size");
+}
+
+bool slab_len(int n) { return n == 64 || n == 96 || n == 128 || n == 160; }
+
+int slab_pitch(int h1) {
+    int p = h1;
+    while (p % 4 != 2) ++p;
+    return p;
+}
+
+size_t slab_smem(int n1, int n2) { return sizeof(float2) * ((size_t)n1 + n2 + (size_t)slab_pitch(n1 / 2 + 1) * n2); }
+
+// ── drivers ──────────────────────────────────────────────────────────────────
+
+BoxMap box_map(const NSPlan& P, const NSBox& b) { return BoxMap{b.nk1, b.nk2, b.b2, P.dims[1]}; }
+
+const NSBox& item_box(const NSPlan& P, int item) {
+    const NSItem& it = P.items_host[item];
+    return P.boxes[it.kind == 1 ? (int)P.boxes.size() - 1 : it.g];
+}
+
+SlabArgs slab_args(const NSPlan& P, const NSBox& b, int nz) {
+    SlabArgs a{};
+    a.P1 = P.P1;
+    a.n3 = P.dims[2];
+    a.nk1 = b.nk1;
+    a.nk2 = b.nk2;
+    a.b2 = b.b2;
+    a.units = nz * P.dims[2];
+    a.twa = P.ffts.at(P.dims[0])->sh.tw;
+    a.twb = P.ffts.at(P.dims[1])->sh.tw;
+    a.es = 1;
+    a.scale = 1.f;
+    return a;
+}
+
+template <bool INV, class Load, class Store>
+void line3(const NSPlan& P, const Load& ld, const Store& so, int nlines, int nz, cudaStream_t st, const char* tag) {
+    const FFTLen* f = P.ffts.at(P.dims[2]).get();
+    if (!launch_reg<INV>(P.dims[2], ld, so, f->sh.tw, nlines, nz, true, st, tag))
+        throw ArgError("no register line pass for axis 3 of this size");
+}
+
+template <int N>
+void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& bx, int i0, int synth, float2* acc,
+                       int nlines, cudaStream_t st) {
+    using Ge = RegGeom<N>;
+    static bool configured = false;
+    if (!configured) {
+        cuda_check(cudaFuncSetAttribute(ns_slab_accum_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)Ge::SMEM),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    dim3 grid((nlines + Ge::LP - 1) / Ge::LP);
+    int tok = prof_begin("ns_slab_accum_axis3", st);
+    ns_slab_accum_kernel<N><<<grid, Ge::THREADS, Ge::SMEM, st>>>(Y, P.SP, nz, P.P1, P.P1 * P.dims[1], bx, P.tb,
+                                                                 P.items.as<NSItem>(), i0, synth, acc,
+                                                                 P.ffts.at(P.dims[2])->sh.tw, nlines);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
+}
+
+// rfft3 of one real channel (element stride es) into the padded spectrum X.
+void slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
+    const NSBox& full = P.boxes_full;
+    SlabArgs a = slab_args(P, full, 1);
+    a.spec = X;
+    a.vol = const_cast<float*>(x);
+    a.es = es;
+    launch_slab<false>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
+                       "ns_slab_r2c");
+    const BoxMap bx = box_map(P, full);
+    const int s3 = P.P1 * P.dims[1];
+    line3<false>(P, L3LoadC{X, 0, P.P1, s3, bx}, L3StoreC{X, 0, P.P1, s3, bx}, full.nk1 * full.nk2, 1, st,
+                 "ns_slab_line3");
+}
+
+// irfft3 of the padded spectrum A (overwritten) into one real channel.
+void slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) {
+    const NSBox& full = P.boxes_full;
+    const BoxMap bx = box_map(P, full);
+    const int s3 = P.P1 * P.dims[1];
+    line3<true>(P, L3LoadC{A, 0, P.P1, s3, bx}, L3StoreC{A, 0, P.P1, s3, bx}, full.nk1 * full.nk2, 1, st,
+                "ns_slab_line3");
+    SlabArgs a = slab_args(P, full, 1);
+    a.spec = A;
+    a.vol = x;
+    a.es = es;
+    a.scale = 1.0f / (float)P.N;
+    launch_slab<true>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
+                      "ns_slab_c2r");
+}
+
+// Analysis of items [i0, i0 + nz) (one mask group) from X into volumes at
+// vol + vz.off(z).
+void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
+                        cudaStream_t st) {
+    const NSBox& b = item_box(P, i0);
+    const BoxMap bx = box_map(P, b);
+    const int s3 = P.P1 * P.dims[1];
+    float2* Y = P.work.as<float2>();
+    line3<true>(P, L3LoadMask{X, P.P1, s3, bx, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0},
+                L3StoreC{Y, P.SP, P.P1, s3, bx}, b.nk1 * b.nk2, nz, st, "ns_slab_mask_axis3");
+    SlabArgs a = slab_args(P, b, nz);
+    a.spec = Y;
+    a.spec_zstride = P.SP;
+    a.vol = vol;
+    a.vz = vz;
+    a.es = es;
+    a.scale = 1.0f / (float)P.N;
+    launch_slab<true>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
+                      "ns_slab_c2r");
+}
+
+// Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
+// vol + vz.off(z) into acc.
+void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                      float2* acc, cudaStream_t st) {
+    const NSBox& b = item_box(P, i0);
+    float2* Y = P.work.as<float2>();
+    SlabArgs a = slab_args(P, b, nz);
+    a.spec = Y;
+    a.spec_zstride = P.SP;
+    a.vol = const_cast<float*>(vol);
+    a.vz = vz;
+    a.es = es;
+    launch_slab<false>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
+                       "ns_slab_r2c");
+    const BoxMap bx = box_map(P, b);
+    const int nl = b.nk1 * b.nk2;
+    const int sy = analysis_masks ? 0 : 1;
+    switch (P.dims[2]) {
+        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+    }
+    throw ArgError("no register line pass for axis 3 of this size");
+}
+
+// Consecutive items of one mask group, at most P.group of them.
+int chunk_end(const NSPlan& P, int i0) {
+    auto key = [&](int i) { return P.items_host[i].kind == 1 ? -1 : P.items_host[i].g; };
+    int i1 = i0 + 1;
+    while (i1 < P.S && i1 - i0 < P.group && key(i1) == key(i0)) ++i1;
+    return i1;
+}
+
+ZMap subband_zmap(const NSPlan& P, int i0, int es) {
+    ZMap zc;
+    zc.items = P.items.as<NSItem>();
+    zc.item0 = i0;
+    zc.sub_stride = P.N * es;
+    return zc;
+}
+
+}  // namespace
+
+bool ns_slab_supported(int n1, int n2, int n3) {
+    return slab_len(n1) && slab_len(n2) && reg_fft_supported(n3) && slab_smem(n1, n2) <= kSlabSmemMax;
+}
+
+// Support box of a table on the rfft grid (h1, n2, n3), k1 fastest.
+NSBox ns_table_box(const std::vector<double>& g, int h1, int n2, int n3) {
+    int m1 = -1, m2 = -1;
+    for (int k3 = 0; k3 < n3; ++k3)
+        for (int k2 = 0; k2 < n2; ++k2) {
+            const double* row = g.data() + (size_t)h1 * (k2 + (size_t)n2 * k3);
+            for (int k1 = 0; k1 < h1; ++k1)
+                if (row[k1] != 0.0) {
+                    m1 = std::max(m1, k1);
+                    m2 = std::max(m2, std::min(k2, n2 - k2));
+                }
+        }
+    return ns_make_box(m1 + 1, m2, n2);
+}
+
+NSBox ns_make_box(int nk1, int b2, int n2) {
+    NSBox b;
+    b.nk1 = std::max(nk1, 1);
+    if (b2 < 0) b2 = 0;
+    if (2 * b2 + 1 >= n2) {
+        b.nk2 = n2;
+        b.b2 = n2;
+    } else {
+        b.nk2 = 2 * b2 + 1;
+        b.b2 = b2;
+    }
+    return b;
+}
+
+void ns_use_slabs(NSPlan& P) {
+    if (!ns_slab_supported(P.dims[0], P.dims[1], P.dims[2]))
+        throw ArgError("the slab pipeline does not support size " + std::to_string(P.dims[0]) + "x" +
+                       std::to_string(P.dims[1]) + "x" + std::to_string(P.dims[2]));
+    P.plane = false;
+    P.slab = true;
+    ns_alloc_scratch(P);
+}
+
+void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
+    const int es = P.nch;
+    float2* X = P.X.as<float2>();
+    for (int ch = 0; ch < P.nch; ++ch) {
+        slab_rfft3(P, reinterpret_cast<const float*>(x) + ch, es, X, st);
+        for (int i0 = 0; i0 < P.S;) {
+            const int i1 = chunk_end(P, i0);
+            slab_analyze_items(P, X, reinterpret_cast<float*>(c) + ch, subband_zmap(P, i0, es), es, i0, i1 - i0,
+                               synth_masks, st);
+            i0 = i1;
+        }
+    }
+}
+
+void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
+    const int es = P.nch;
+    float2* A = P.acc.as<float2>();
+    for (int ch = 0; ch < P.nch; ++ch) {
+        cuda_check(cudaMemsetAsync(A, 0, sizeof(float2) * P.SP, st), "cudaMemsetAsync(acc)");
+        for (int i0 = 0; i0 < P.S;) {
+            const int i1 = chunk_end(P, i0);
+            slab_synth_items(P, reinterpret_cast<const float*>(c) + ch, subband_zmap(P, i0, es), es, i0, i1 - i0,
+                             analysis_masks, A, st);
+            i0 = i1;
+        }
+        slab_irfft3(P, A, reinterpret_cast<float*>(x) + ch, es, st);
+    }
+}
+
+void ns_slab_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
+    for (int ch = 0; ch < P.nch; ++ch)
+        slab_rfft3(P, reinterpret_cast<const float*>(x) + ch, P.nch, P.X.as<float2>() + ch * P.SP, st);
+}
+
+void ns_slab_stream_analyze_one(NSPlan& P, int pos, void* band, cudaStream_t st) {
+    for (int ch = 0; ch < P.nch; ++ch)
+        slab_analyze_items(P, P.X.as<float2>() + ch * P.SP, reinterpret_cast<float*>(band) + ch, ZMap{}, P.nch, pos,
+                           1, false, st);
+}
+
+void ns_slab_stream_synth_push(NSPlan& P, int pos, const void* band, cudaStream_t st) {
+    if (pos == 0)
+        cuda_check(cudaMemsetAsync(P.acc.p, 0, sizeof(float2) * P.SP * P.nch, st), "cudaMemsetAsync(acc)");
+    for (int ch = 0; ch < P.nch; ++ch)
+        slab_synth_items(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, pos, 1, false,
+                         P.acc.as<float2>() + ch * P.SP, st);
+}
+
+void ns_slab_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
+    for (int ch = 0; ch < P.nch; ++ch)
+        slab_irfft3(P, P.acc.as<float2>() + ch * P.SP, reinterpret_cast<float*>(x) + ch, P.nch, st);
+}
+
+}  // namespace sfl

@@ -79,6 +79,12 @@ struct NSMaskTables {
     int low_off[3] = {0, 0, 0};
 };
 
+// Support box of a mask group on the rfft grid: rows k1 < nk1 and the nk2
+// columns |k2| <= b2 (k2 <= b2 or k2 >= n2 - b2; b2 >= n2 when all).
+struct NSBox {
+    int nk1 = 0, nk2 = 0, b2 = 0;
+};
+
 struct NSPlan {
     sfl_ns_params p{};
     int dims[3] = {0, 0, 0};
@@ -97,6 +103,13 @@ struct NSPlan {
     DevMem Gp, Blp;         // G and Bl in plane-major order
     NSMaskTables tbp;
     DevMem status;          // device status word of bounded waits (0 = fine)
+    // slab pipeline (spectra with the axis-1 pitch padded to P1)
+    bool slab = false;
+    int P1 = 0;
+    long long SP = 0;               // P1 * n2 * n3
+    std::vector<NSBox> boxes;       // per mask group, then the lowpass
+    NSBox boxes_full;
+    int sms = 148;
     std::map<int, std::unique_ptr<FFTLen>> ffts;
     DevMem X;        // nch spectra
     DevMem work;     // group spectra
@@ -137,6 +150,18 @@ void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
 // Plane-major pipeline (ns_plane.cu).
 bool ns_plane_supported(int n1, int n2, int n3);
 void ns_use_planes(NSPlan& P);
+// Slab pipeline (ns_slab.cu).
+bool ns_slab_supported(int n1, int n2, int n3);
+void ns_use_slabs(NSPlan& P);
+NSBox ns_make_box(int nk1, int b2, int n2);
+NSBox ns_table_box(const std::vector<double>& g, int h1, int n2, int n3);
+void ns_alloc_scratch(NSPlan& P);
+void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
+void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
+void ns_slab_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);
+void ns_slab_stream_analyze_one(NSPlan& P, int pos, void* band, cudaStream_t st);
+void ns_slab_stream_synth_push(NSPlan& P, int pos, const void* band, cudaStream_t st);
+void ns_slab_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
 void ns_plane_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
 void ns_plane_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
 void ns_plane_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);

@@ -335,10 +335,11 @@ class Workspace:
     def set_group(self, group):
         check(lib.sfl_plan_set_group(self._h, int(group)))
 
-    PIPELINES = {"lines": 0, "planes": 1}
+    PIPELINES = {"lines": 0, "planes": 1, "slabs": 2}
 
     def set_pipeline(self, name):
-        """NSSurfacelet kernel pipeline: "lines" (default) or "planes"."""
+        """NSSurfacelet kernel pipeline: "slabs" (the default where the size
+        allows), "lines" or "planes"."""
         if name not in self.PIPELINES:
             raise ArgumentError(f"unknown pipeline {name!r}; expected one of {sorted(self.PIPELINES)}")
         check(lib.sfl_plan_set_pipeline(self._h, self.PIPELINES[name]))

@@ -34,12 +34,14 @@ CASES = [
     ((32, 32, 32), dict(scales=3, direction_levels=[2, 2, 3])),
     ((26, 30, 12), dict(scales=1, direction_levels=[3], bernstein_order=6, transition=0.5)),
     ((16, 12, 20), dict(scales=2, direction_levels=[1, 2], bernstein_order=6, tight=False)),
-    # sizes the plane-major pipeline also supports
+    # sizes the slab and plane-major pipelines also support
     ((64, 64, 64), dict(scales=3, direction_levels=[2, 2, 3])),
     ((96, 64, 128), dict(scales=2, direction_levels=[1, 3], bernstein_order=6)),
     ((128, 128, 64), dict(scales=2, direction_levels=[2, 2], bernstein_order=8, tight=False)),
+    ((64, 96, 32), dict(scales=3, direction_levels=[1, 2, 2], bernstein_order=8)),
 ]
-PIPELINE_CASES = [(d, k, "lines") for d, k in CASES] + [(d, k, "planes") for d, k in CASES[-3:]]
+PIPELINE_CASES = ([(d, k, "lines") for d, k in CASES] + [(d, k, "planes") for d, k in CASES[-4:-1]]
+                  + [(d, k, "slabs") for d, k in CASES[-4:]])
 
 
 @pytest.mark.parametrize("dims,kw,pipeline", PIPELINE_CASES)
@@ -140,8 +142,8 @@ def test_streaming_matches_materialized(sfl):
         sfl.synthesize_(lambda i: sfl.volume_like((4, 4, 4)), sfl.volume_like(dims), ws)
 
 
-@pytest.mark.parametrize("dims,pipeline", [((64, 64, 64), "lines"), ((64, 64, 64), "planes"),
-                                           ((16, 16, 16), "lines")])
+@pytest.mark.parametrize("dims,pipeline", [((64, 64, 64), "slabs"), ((64, 64, 64), "lines"),
+                                           ((64, 64, 64), "planes"), ((16, 16, 16), "lines")])
 @pytest.mark.parametrize("dtype", ["float32", "complex64"])
 def test_streaming_equals_materialized_bit_for_bit(sfl, dims, pipeline, dtype):
     # test/items/test_ns_surfacelet.jl:79-106, 108-138
@@ -180,8 +182,10 @@ def test_pipeline_selection_is_validated(sfl):
     ws = sfl.make_workspace(sfl.NSSurfacelet(scales=1, direction_levels=[1], bernstein_order=4), "float32", (12, 10, 8))
     with pytest.raises(sfl.ArgumentError, match="plane-major pipeline does not support"):
         ws.set_pipeline("planes")
+    with pytest.raises(sfl.ArgumentError, match="slab pipeline does not support"):
+        ws.set_pipeline("slabs")
     with pytest.raises(sfl.ArgumentError, match="unknown pipeline"):
-        ws.set_pipeline("slabs?")
+        ws.set_pipeline("pencils")
     ws.set_pipeline("lines")
 
 
