@@ -258,11 +258,13 @@ def main():
     buf = C.create_string_buffer(4096)
     lib.sfl_profile_tags(buf, 4096)
     tags = [s for s in buf.value.decode().split("\n") if s]
-    per_tag = {}
+    per_tag, tag_bytes = {}, {}
     for tg in tags:
-        tot, cnt = C.c_double(), C.c_int64()
+        tot, cnt, nb = C.c_double(), C.c_int64(), C.c_double()
         lib.sfl_profile_read(tg.encode(), C.byref(tot), C.byref(cnt))
+        lib.sfl_profile_bytes(tg.encode(), C.byref(nb))
         per_tag[tg] = (tot.value / prof_steps, cnt.value // prof_steps)
+        tag_bytes[tg] = nb.value / prof_steps
     lib.sfl_profile_reset()
     launches_per_step = sum(c for _, c in per_tag.values())
     dom = max(per_tag, key=lambda k: per_tag[k][0])
@@ -276,7 +278,7 @@ def main():
         "ns_c2c_axis3": B * 3, "ns_mask_axis3": B * 2 * S, "ns_accum_axis3": B * S,
     }.get(dom, 0)
     hbm, peak_kind = peaks()
-    alg = kernel_bytes(dom, None, dom_launches, nz_total)
+    alg = tag_bytes.get(dom) or kernel_bytes(dom, None, dom_launches, nz_total)
     achieved = alg / (dom_ms / 1e3) / 1e9 if alg else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
@@ -304,6 +306,8 @@ def main():
         "op_roofline": {"algorithmic_bytes_per_voxel": 600, "achieved_gbs": op_bytes / (ms / 1e3) / 1e9 / world,
                         "frac": op_bytes / (ms / 1e3) / 1e9 / world / hbm, "peak_kind": peak_kind},
         "kernel_ms_per_step": {k: v[0] for k, v in per_tag.items()},
+        "kernel_algorithmic_gbs": {k: tag_bytes[k] / (v[0] / 1e3) / 1e9 for k, v in per_tag.items()
+                                   if tag_bytes.get(k)},
     }
     if clk:
         line["clocks"] = {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}

@@ -238,6 +238,24 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
 int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name,
                           int32_t index, double* out, int64_t* count);
 
+/* ── Batches ─────────────────────────────────────────────────────────────
+ * Many transforms as one CUDA graph: batch_create runs each (plan, input,
+ * output) once eagerly, then captures the sequence (distinct plans on up to
+ * four concurrent branches; transforms of one plan keep their order) and
+ * instantiates it; batch_run replays it on a stream with the same pointers,
+ * whose contents may change between runs.  The plans must stay alive and
+ * must not be used elsewhere while a run is in flight.  No counterpart in the
+ * reference, whose batches are loops of plain calls. */
+typedef struct sfl_batch sfl_batch;
+#define SFL_OP_ANALYZE 0
+#define SFL_OP_SYNTHESIZE 1
+#define SFL_OP_ADJOINT_ANALYZE 2
+#define SFL_OP_ADJOINT_SYNTHESIZE 3
+int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* inputs, void* const* outputs,
+                     int32_t op, sfl_batch** out);
+int sfl_batch_run(sfl_batch* batch, void* stream);
+int sfl_batch_destroy(sfl_batch* batch);
+
 /* ── Launch timing (benchmark instrumentation) ───────────────────────────
  * No counterpart in the reference.  While enabled, every kernel launch of the
  * library is bracketed by two CUDA events on its stream and filed under its
@@ -247,6 +265,10 @@ int sfl_profile_enable(int32_t on);
 int sfl_profile_reset(void);
 int sfl_profile_read(const char* tag, double* total_ms, int64_t* launches);
 int sfl_profile_tags(char* buf, int64_t cap);
+/* Algorithmic bytes (each input read once, each output written once) of the
+ * profiled launches of a tag (all tags when tag is NULL), where the launch
+ * site reports them. */
+int sfl_profile_bytes(const char* tag, double* bytes);
 
 #ifdef __cplusplus
 }

@@ -8,6 +8,7 @@ reference's AbstractMultiscaleTransforms interface over it.  There is no CPU
 fallback: importing the package fails if the library is missing.
 """
 
+from .batch import Batch  # noqa: F401
 from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateError, lib  # noqa: F401
 from .transforms import (  # noqa: F401
     NSSurfacelet, Surfacelet, Workspace, adjoint_analyze, adjoint_analyze_, adjoint_synthesize,

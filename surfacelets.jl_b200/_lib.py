@@ -88,6 +88,15 @@ SIGNATURES = {
                                       C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "sfl_surf_design_table": (C.c_int, [C.POINTER(SurfParams), Dims, C.c_char_p, C.c_int32,
                                         C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "sfl_batch_create": (C.c_int, [C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.c_int32,
+                                   C.POINTER(P)]),
+    "sfl_batch_run": (C.c_int, [P, P]),
+    "sfl_batch_destroy": (C.c_int, [P]),
+    "sfl_profile_enable": (C.c_int, [C.c_int32]),
+    "sfl_profile_reset": (C.c_int, []),
+    "sfl_profile_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "sfl_profile_tags": (C.c_int, [C.c_char_p, C.c_int64]),
+    "sfl_profile_bytes": (C.c_int, [C.c_char_p, C.POINTER(C.c_double)]),
 }
 
 

@@ -1,14 +1,18 @@
 // extern "C" entry points of libsurfacelets_b200.so (declared in
 // include/surfacelets_b200.h).  Every entry point catches the library's
 // exceptions and turns them into a status code plus a thread-local message.
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/surfacelets_b200.h"
 #include "design.h"
 #include "plan.h"
+#include "prof.h"
 
 namespace sfl {
 
@@ -107,7 +111,38 @@ void on_device(const sfl_plan* plan, F&& f) {
     if (cur != plan->impl.device) sfl::cuda_check(cudaSetDevice(cur), "cudaSetDevice");
 }
 
+// One transform of a plan (the four operators of the C ABI).
+void run_op(sfl_plan* plan, int op, const void* in, void* out, cudaStream_t st) {
+    sfl::Plan& P = plan->impl;
+    const bool ns = P.kind == SFL_KIND_NS;
+    switch (op) {
+        case SFL_OP_ANALYZE:
+            ns ? sfl::ns_analyze(*P.ns, in, out, st, false) : sfl::dec_analyze(*P.dec, in, out, st);
+            return;
+        case SFL_OP_SYNTHESIZE:
+            ns ? sfl::ns_synthesize(*P.ns, in, out, st, false) : sfl::dec_synthesize(*P.dec, in, out, st);
+            return;
+        case SFL_OP_ADJOINT_ANALYZE:
+            ns ? sfl::ns_synthesize(*P.ns, in, out, st, true) : sfl::dec_adjoint_analyze(*P.dec, in, out, st);
+            return;
+        case SFL_OP_ADJOINT_SYNTHESIZE:
+            ns ? sfl::ns_analyze(*P.ns, in, out, st, true) : sfl::dec_adjoint_synthesize(*P.dec, in, out, st);
+            return;
+    }
+    throw sfl::ArgError("unknown operator " + std::to_string(op));
+}
+
 }  // namespace
+
+struct sfl_batch {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+    ~sfl_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
 
 extern "C" {
 
@@ -606,6 +641,117 @@ int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const
         }
         *count = (int64_t)tmp.size();
         if (out) std::memcpy(out, tmp.data(), sizeof(double) * tmp.size());
+        return SFL_OK;
+    });
+}
+
+// ── batches: one CUDA graph over many transforms ─────────────────────────────
+
+int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* inputs, void* const* outputs,
+                     int32_t op, sfl_batch** out) {
+    return guarded([&] {
+        need(plans, "plans");
+        need(inputs, "inputs");
+        need(outputs, "outputs");
+        need(out, "out");
+        *out = nullptr;
+        if (n < 1) throw sfl::ArgError("a batch needs at least one transform, got " + std::to_string(n));
+        if (op < SFL_OP_ANALYZE || op > SFL_OP_ADJOINT_SYNTHESIZE)
+            throw sfl::ArgError("unknown operator " + std::to_string(op));
+        const int dev = (need(plans[0], "plans[0]"), plans[0]->impl.device);
+        // distinct plans run on up to kBranches concurrent branches; one plan always on the same branch
+        constexpr int kBranches = 4;
+        std::vector<const sfl_plan*> distinct;
+        std::vector<int> branch(n);
+        for (int i = 0; i < n; ++i) {
+            need(plans[i], "plans[i]");
+            need(inputs[i], "inputs[i]");
+            need(outputs[i], "outputs[i]");
+            if (plans[i]->impl.device != dev) throw sfl::ArgError("the plans of a batch must share one device");
+            if (plans[i]->impl.kind == SFL_KIND_NS && plans[i]->impl.ns->stream_mode != 0)
+                throw sfl::ArgError("a streaming pass is open on a plan of the batch");
+            check_aligned(inputs[i], plans[i]->impl.dtype, "inputs[i]");
+            check_aligned(outputs[i], plans[i]->impl.dtype, "outputs[i]");
+            auto it = std::find(distinct.begin(), distinct.end(), plans[i]);
+            if (it == distinct.end()) {
+                distinct.push_back(plans[i]);
+                it = distinct.end() - 1;
+            }
+            branch[i] = (int)(it - distinct.begin()) % kBranches;
+        }
+        std::unique_ptr<sfl_batch> b(new sfl_batch());
+        b->device = dev;
+        on_device(plans[0], [&] {
+            cudaStream_t s[kBranches] = {};
+            cudaEvent_t fork = nullptr, join[kBranches] = {};
+            auto cleanup = [&] {
+                for (auto& e : join)
+                    if (e) cudaEventDestroy(e);
+                if (fork) cudaEventDestroy(fork);
+                for (auto& x : s)
+                    if (x) cudaStreamDestroy(x);
+            };
+            const bool prof = sfl::prof_on();
+            try {
+                for (auto& x : s) sfl::cuda_check(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "stream");
+                sfl::cuda_check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+                for (auto& e : join) sfl::cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+                // one eager pass: validates the arguments and configures every kernel outside the capture
+                for (int i = 0; i < n; ++i) run_op(plans[i], op, inputs[i], outputs[i], s[0]);
+                sfl::cuda_check(cudaStreamSynchronize(s[0]), "batch warm-up");
+                sfl_profile_enable(0);
+                sfl::cuda_check(cudaStreamBeginCapture(s[0], cudaStreamCaptureModeThreadLocal), "begin capture");
+                try {
+                    sfl::cuda_check(cudaEventRecord(fork, s[0]), "fork");
+                    for (int k = 1; k < kBranches; ++k) sfl::cuda_check(cudaStreamWaitEvent(s[k], fork, 0), "fork");
+                    for (int i = 0; i < n; ++i) run_op(plans[i], op, inputs[i], outputs[i], s[branch[i]]);
+                    for (int k = 1; k < kBranches; ++k) {
+                        sfl::cuda_check(cudaEventRecord(join[k], s[k]), "join");
+                        sfl::cuda_check(cudaStreamWaitEvent(s[0], join[k], 0), "join");
+                    }
+                } catch (...) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(s[0], &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                sfl::cuda_check(cudaStreamEndCapture(s[0], &b->graph), "end capture");
+                sfl::cuda_check(cudaGraphInstantiate(&b->exec, b->graph, 0), "cudaGraphInstantiate");
+                sfl_profile_enable(prof ? 1 : 0);
+            } catch (...) {
+                sfl_profile_enable(prof ? 1 : 0);
+                cleanup();
+                throw;
+            }
+            cleanup();
+        });
+        *out = b.release();
+        return SFL_OK;
+    });
+}
+
+int sfl_batch_run(sfl_batch* batch, void* stream) {
+    return guarded([&] {
+        need(batch, "batch");
+        int cur = 0;
+        sfl::cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
+        if (cur != batch->device) sfl::cuda_check(cudaSetDevice(batch->device), "cudaSetDevice");
+        cudaError_t e = cudaGraphLaunch(batch->exec, as_stream(stream));
+        if (cur != batch->device) cudaSetDevice(cur);
+        sfl::cuda_check(e, "cudaGraphLaunch");
+        return SFL_OK;
+    });
+}
+
+int sfl_batch_destroy(sfl_batch* batch) {
+    return guarded([&] {
+        if (!batch) return SFL_OK;
+        int cur = 0;
+        const int dev = batch->device;
+        sfl::cuda_check(cudaGetDevice(&cur), "cudaGetDevice");
+        if (cur != dev) cudaSetDevice(dev);
+        delete batch;
+        if (cur != dev) cudaSetDevice(cur);
         return SFL_OK;
     });
 }

@@ -126,8 +126,12 @@ __global__ void hg_mask_kernel(const float2* X, int n0, int n1, float2* S, int h
 // the 2b-bin groups along axis m, analysis A <- F0(A)A + F0(B)B,
 // B <- F1(A)A + F1(B)B; synthesis A <- G0(A)A + G1(A)B, B <- G0(B)A + G1(B)B.
 // src/directional/irc.jl:304-345 (file numbering)
+// With conj, the coefficients enter conjugated (the adjoint of a stage is its
+// conjugate transpose: the analysis adjoint takes the synthesis form with
+// conj(F0), conj(F1); the synthesis adjoint the analysis form with conj(G0),
+// conj(G1)).
 __global__ void irc_stage_kernel(float2* S, int h0, int h1, int h2, int K, int m, int b, const float2* f0,
-                                 const float2* f1, int synth) {
+                                 const float2* f1, int synth, int conj) {
     int hd[3] = {h0, h1, h2};
     int pd[3] = {h0, h1, h2};
     pd[m] = hd[m] / 2;
@@ -150,13 +154,20 @@ __global__ void irc_stage_kernel(float2* S, int h0, int h1, int h2, int K, int m
         int kK = c[K];
         long long fA = kK + (long long)nKh * cA, fB = kK + (long long)nKh * cB;
         float2 A = S[aA], Bv = S[aB];
+        float2 f0A = f0[fA], f0B = f0[fB], f1A = f1[fA], f1B = f1[fB];
+        if (conj) {
+            f0A.y = -f0A.y;
+            f0B.y = -f0B.y;
+            f1A.y = -f1A.y;
+            f1B.y = -f1B.y;
+        }
         float2 nA, nB;
         if (!synth) {
-            nA = c_add(c_mul(f0[fA], A), c_mul(f0[fB], Bv));
-            nB = c_add(c_mul(f1[fA], A), c_mul(f1[fB], Bv));
+            nA = c_add(c_mul(f0A, A), c_mul(f0B, Bv));
+            nB = c_add(c_mul(f1A, A), c_mul(f1B, Bv));
         } else {
-            nA = c_add(c_mul(f0[fA], A), c_mul(f1[fA], Bv));
-            nB = c_add(c_mul(f0[fB], A), c_mul(f1[fB], Bv));
+            nA = c_add(c_mul(f0A, A), c_mul(f1A, Bv));
+            nB = c_add(c_mul(f0B, A), c_mul(f1B, Bv));
         }
         S[aA] = nA;
         S[aB] = nB;
@@ -195,6 +206,64 @@ __global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs
         }
         X[q] = v;
     }
+}
+
+// Adjoint of the hourglass masks of the analysis: X = sum_K pad_K(V_K s_K S_K),
+// zero outside each half grid.
+__global__ void hg_adjoint_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs ha, float s0, float s1, float s2) {
+    long long total = (long long)n0 * n1 * n2;
+    int n[3] = {n0, n1, n2};
+    const float sK[3] = {s0, s1, s2};
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int k[3];
+        k[0] = q % n0;
+        long long r = q / n0;
+        k[1] = r % n1;
+        k[2] = r / n1;
+        float2 v = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int K = 0; K < 3; ++K) {
+            int hd[3] = {n0, n1, n2};
+            hd[K] = n[K] / 2 + 1;
+            if (k[K] < hd[K]) {
+                long long a = lin3(k[0], k[1], k[2], hd[0], hd[1]);
+                v = c_add(v, c_scale(ha.S[K][a], sK[K] * ha.V[K][a]));
+            }
+        }
+        X[q] = v;
+    }
+}
+
+// Adjoint of the Hermitian sum of the synthesis, for hourglass K: on its half
+// grid S_K[a] = (1/3) V_K[a] (X[a] + conj(X[-a]) where -a lies outside the
+// half grid along K).
+__global__ void herm_gather_kernel(const float2* X, int n0, int n1, int n2, float2* S, const float* V, int K,
+                                   float third) {
+    int n[3] = {n0, n1, n2};
+    int hd[3] = {n0, n1, n2};
+    hd[K] = n[K] / 2 + 1;
+    long long total = (long long)hd[0] * hd[1] * hd[2];
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+         q += (long long)gridDim.x * blockDim.x) {
+        int a[3];
+        a[0] = q % hd[0];
+        long long r = q / hd[0];
+        a[1] = r % hd[1];
+        a[2] = r / hd[1];
+        float2 v = X[lin3(a[0], a[1], a[2], n0, n1)];
+        const int mK = (n[K] - a[K]) % n[K];
+        if (mK >= hd[K]) {
+            int m0 = (n0 - a[0]) % n0, m1 = (n1 - a[1]) % n1, m2 = (n2 - a[2]) % n2;
+            v = c_add(v, c_conj(X[lin3(m0, m1, m2, n0, n1)]));
+        }
+        S[q] = c_scale(v, third * V[q]);
+    }
+}
+
+__global__ void cscale_kernel(float2* X, long long n, float s) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        X[q] = c_scale(X[q], s);
 }
 
 // Block <-> subband address map of hourglass K at one level.  Line l of S_K
@@ -520,7 +589,9 @@ Lines k_lines(const DecLevelDev& L, int K) {
     return g;
 }
 
-void pyr_split(DecPlan& D, int j, cudaStream_t st) {
+// Split of level j; with adjoint, the adjoint of the merge (the same gather
+// with the merge's D^1.5 weights).
+void pyr_split(DecPlan& D, int j, cudaStream_t st, bool adjoint = false) {
     DecLevelDev& L = *D.lv[j];
     float2* X = D.spectra[j]->as<float2>();
     float2* low = D.spectra[j + 1]->as<float2>();
@@ -530,14 +601,16 @@ void pyr_split(DecPlan& D, int j, cudaStream_t st) {
         int tok = prof_begin("dec_pyr_split", st);
         pyr_split_kernel<<<grid_for(tot), 256, 0, st>>>(
             X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
-            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.lw_split.as<float>(),
-            L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
+            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(),
+            adjoint ? L.lw_merge.as<float>() : L.lw_split.as<float>(), L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
         prof_end(tok, st);
     }
     cuda_check(cudaGetLastError(), "pyr_split_kernel");
 }
 
-void pyr_merge(DecPlan& D, int j, cudaStream_t st) {
+// Merge of level j; with adjoint, the adjoint of the split (the same scatter
+// with the split's D^-1.5 weights).
+void pyr_merge(DecPlan& D, int j, cudaStream_t st, bool adjoint = false) {
     DecLevelDev& L = *D.lv[j];
     float2* X = D.spectra[j]->as<float2>();
     const float2* low = D.spectra[j + 1]->as<float2>();
@@ -546,8 +619,8 @@ void pyr_merge(DecPlan& D, int j, cudaStream_t st) {
         int tok = prof_begin("dec_pyr_merge", st);
         pyr_merge_kernel<<<grid_for(tot), 256, 0, st>>>(
             X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
-            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(), L.lw_merge.as<float>(),
-            L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
+            L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(),
+            adjoint ? L.lw_split.as<float>() : L.lw_merge.as<float>(), L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
         prof_end(tok, st);
     }
     cuda_check(cudaGetLastError(), "pyr_merge_kernel");
@@ -574,7 +647,7 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
             {
                 int tok = prof_begin("dec_irc", st);
                 irc_stage_kernel<<<grid_for(pairs), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
-                                                                  sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0);
+                                                                  sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0, 0);
                 prof_end(tok, st);
             }
             cuda_check(cudaGetLastError(), "irc_stage_kernel");
@@ -618,7 +691,7 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
             {
                 int tok = prof_begin("dec_irc", st);
                 irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
-                                                                    sg.f[2].as<float2>(), sg.f[3].as<float2>(), 1);
+                                                                    sg.f[2].as<float2>(), sg.f[3].as<float2>(), 1, 0);
                 prof_end(tok, st);
             }
             cuda_check(cudaGetLastError(), "irc_stage_kernel");
@@ -634,6 +707,100 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
         prof_end(tok, st);
     }
     cuda_check(cudaGetLastError(), "hermitian_sum_kernel");
+}
+
+// Adjoint of scale_forward: the subbands of level j (real, in c) to the
+// level's spectrum.  Per hourglass: a_k * R2C along K (a_k = 2 off the
+// self-conjugate bins: the adjoint of the C2R), forward block FFTs (adjoint of
+// the backward ones), the IRC stages in reverse order conjugate-transposed;
+// then the zero-padded sum of V_K s_K S_K.
+void scale_forward_adjoint(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    HermArgs ha;
+    float sK[3];
+    for (int K = 0; K < 3; ++K) {
+        const int* hd = L.hd[K];
+        float2* S = D.S[K].as<float2>();
+        Lines gk = k_lines(L, K);
+        FFTLen* f = get_fft(D.ffts, L.n[K]);
+        BlockMap bm = block_map(L, K);
+        int pairs = (gk.nlines + 1) / 2;
+        if (!launch_reg<false>(L.n[K], RLoadRPairBlocks{c, bm, gk.nlines, es},
+                               RStoreHalfPair{S, ZMap{}, gk, L.n[K], 2.f}, f->sh.tw, pairs, 1, K != 0, st,
+                               "dec_r2c_blocks")) {
+            LoadRPairBlocks ld{c, bm, gk.nlines, es};
+            StoreHalfPair sto{S, ZMap{}, gk, 2.f};
+            launch_pass(ld, sto, f->sh, pairs, 1, false, st, "dec_r2c_blocks");
+        }
+        for (int m = 0; m < 3; ++m)
+            if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
+        long long tot = (long long)hd[0] * hd[1] * hd[2];
+        for (int sg_i = (int)L.stages[K].size() - 1; sg_i >= 0; --sg_i) {
+            auto& sg = L.stages[K][sg_i];
+            int tok = prof_begin("dec_irc", st);
+            irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                                                                sg.f[0].as<float2>(), sg.f[1].as<float2>(), 1, 1);
+            prof_end(tok, st);
+            cuda_check(cudaGetLastError(), "irc_stage_kernel");
+        }
+        int sb[3];
+        for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
+        sK[K] = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
+        ha.S[K] = S;
+        ha.V[K] = L.V[K].as<float>();
+    }
+    long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
+    int tok = prof_begin("dec_hg_adjoint", st);
+    hg_adjoint_sum_kernel<<<grid_for(tot), 256, 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
+                                                          sK[0], sK[1], sK[2]);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "hg_adjoint_sum_kernel");
+}
+
+// Adjoint of scale_inverse: the level's spectrum to its subbands.  Per
+// hourglass: the gather adjoint to the Hermitian sum, the synthesis IRC
+// stages in forward order conjugate-transposed, backward block FFTs, and the
+// C2R along K of S / a_k (the adjoint of the R2C).
+void scale_inverse_adjoint(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    for (int K = 0; K < 3; ++K) {
+        const int* hd = L.hd[K];
+        float2* S = D.S[K].as<float2>();
+        long long tot = (long long)hd[0] * hd[1] * hd[2];
+        {
+            int tok = prof_begin("dec_herm_gather", st);
+            herm_gather_kernel<<<grid_for(tot), 256, 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], S,
+                                                               L.V[K].as<float>(), K, 1.0f / 3.0f);
+            prof_end(tok, st);
+            cuda_check(cudaGetLastError(), "herm_gather_kernel");
+        }
+        for (auto& sg : L.stages[K]) {
+            int tok = prof_begin("dec_irc", st);
+            irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                                                                sg.f[2].as<float2>(), sg.f[3].as<float2>(), 0, 1);
+            prof_end(tok, st);
+            cuda_check(cudaGetLastError(), "irc_stage_kernel");
+        }
+        for (int m = 0; m < 3; ++m)
+            if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], true, st);
+        Lines gk = k_lines(L, K);
+        FFTLen* f = get_fft(D.ffts, L.n[K]);
+        BlockMap bm = block_map(L, K);
+        int pairs = (gk.nlines + 1) / 2;
+        if (!launch_reg<true>(L.n[K], RLoadHPair{S, ZMap{}, gk, L.n[K], 0.5f}, RStoreRPairBlocks{c, bm, gk.nlines, es},
+                              f->sh.tw, pairs, 1, K != 0, st, "dec_c2r_blocks")) {
+            LoadHPair ld{S, ZMap{}, gk, 0.5f};
+            StoreRPairBlocks sto{c, bm, gk.nlines, es};
+            launch_pass(ld, sto, f->sh, pairs, 1, true, st, "dec_c2r_blocks");
+        }
+    }
+}
+
+void cscale(float2* X, long long n, float s, cudaStream_t st) {
+    int tok = prof_begin("dec_scale", st);
+    cscale_kernel<<<grid_for(n), 256, 0, st>>>(X, n, s);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "cscale_kernel");
 }
 
 }  // namespace
@@ -672,12 +839,49 @@ void dec_synthesize(DecPlan& D, const void* c, void* x, cudaStream_t st) {
     }
 }
 
-void dec_adjoint_analyze(DecPlan&, const void*, void*, cudaStream_t) {
-    throw ArgError("the adjoint of the decimated transform is not available in this build");
+// x = A^T c, the adjoint of dec_analyze under the real inner products of the
+// volume and the coefficient vector: every stage of the analysis replaced by
+// its adjoint, in reverse order (FFT -> Re(bfft), split -> merge with the
+// split weights, hourglass mask -> zero-padded V_K s, IRC -> conjugate
+// transpose, backward block FFT -> forward, C2R -> a_k R2C, the lowpass's
+// Re(bfft)/M -> FFT/M).
+void dec_adjoint_analyze(DecPlan& D, const void* c, void* x, cudaStream_t st) {
+    const int es = D.nch;
+    const SurfDesign& S = D.design;
+    for (int ch = 0; ch < D.nch; ++ch) {
+        const float* cin = reinterpret_cast<const float*>(c) + ch;
+        float* xout = reinterpret_cast<float*>(x) + ch;
+        const int* nl = S.pyramid[D.J - 1].nlow;
+        const long long M = (long long)nl[0] * nl[1] * nl[2];
+        fft_real_full(D, cin, es, nl, D.spectra[D.J]->as<float2>(), st);
+        cscale(D.spectra[D.J]->as<float2>(), M, (float)(1.0 / (double)M), st);
+        for (int j = D.J - 1; j >= 0; --j) {
+            scale_forward_adjoint(D, j, cin, es, st);
+            pyr_merge(D, j, st, true);
+        }
+        ifft_full_real(D, D.spectra[0]->as<float2>(), D.dims, xout, es, 1.0f, st);
+    }
 }
 
-void dec_adjoint_synthesize(DecPlan&, const void*, void*, cudaStream_t) {
-    throw ArgError("the adjoint of the decimated transform is not available in this build");
+// c = S^T x, the adjoint of dec_synthesize: FFT/N of x, then per level the
+// adjoint of the merge (a split with the merge weights) and of the scale's
+// inverse, and Re(bfft) of the coarse spectrum into the lowpass.
+void dec_adjoint_synthesize(DecPlan& D, const void* x, void* c, cudaStream_t st) {
+    const int es = D.nch;
+    const SurfDesign& S = D.design;
+    for (int ch = 0; ch < D.nch; ++ch) {
+        const float* xin = reinterpret_cast<const float*>(x) + ch;
+        float* cout = reinterpret_cast<float*>(c) + ch;
+        const long long N = (long long)D.dims[0] * D.dims[1] * D.dims[2];
+        fft_real_full(D, xin, es, D.dims, D.spectra[0]->as<float2>(), st);
+        cscale(D.spectra[0]->as<float2>(), N, (float)(1.0 / (double)N), st);
+        for (int j = 0; j < D.J; ++j) {
+            pyr_split(D, j, st, true);
+            scale_inverse_adjoint(D, j, cout, es, st);
+        }
+        const int* nl = S.pyramid[D.J - 1].nlow;
+        ifft_full_real(D, D.spectra[D.J]->as<float2>(), nl, cout, es, 1.0f, st);
+    }
 }
 
 }  // namespace sfl

@@ -580,9 +580,14 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
     cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
 }
 
+// Algorithmic bytes of one box of a spectrum (complex float32 bins).
+double box_bytes(const NSPlan& P, const NSBox& b) { return 8.0 * b.nk1 * b.nk2 * P.dims[2]; }
+
 // rfft3 of one real channel (element stride es) into the padded spectrum X.
 void slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
     const NSBox& full = P.boxes_full;
+    prof_bytes("ns_slab_r2c", 4.0 * P.N + box_bytes(P, full));
+    prof_bytes("ns_slab_line3", 2 * box_bytes(P, full));
     SlabArgs a = slab_args(P, full, 1);
     a.spec = X;
     a.vol = const_cast<float*>(x);
@@ -598,6 +603,8 @@ void slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
 // irfft3 of the padded spectrum A (overwritten) into one real channel.
 void slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) {
     const NSBox& full = P.boxes_full;
+    prof_bytes("ns_slab_line3", 2 * box_bytes(P, full));
+    prof_bytes("ns_slab_c2r", box_bytes(P, full) + 4.0 * P.N);
     const BoxMap bx = box_map(P, full);
     const int s3 = P.P1 * P.dims[1];
     line3<true>(P, L3LoadC{A, 0, P.P1, s3, bx}, L3StoreC{A, 0, P.P1, s3, bx}, full.nk1 * full.nk2, 1, st,
@@ -619,6 +626,9 @@ void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es,
     const BoxMap bx = box_map(P, b);
     const int s3 = P.P1 * P.dims[1];
     float2* Y = P.work.as<float2>();
+    // X and the group table once, the nz spectra out; then those back in and nz volumes out
+    prof_bytes("ns_slab_mask_axis3", 1.5 * box_bytes(P, b) + nz * box_bytes(P, b));
+    prof_bytes("ns_slab_c2r", nz * (box_bytes(P, b) + 4.0 * P.N));
     line3<true>(P, L3LoadMask{X, P.P1, s3, bx, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0},
                 L3StoreC{Y, P.SP, P.P1, s3, bx}, b.nk1 * b.nk2, nz, st, "ns_slab_mask_axis3");
     SlabArgs a = slab_args(P, b, nz);
@@ -638,6 +648,9 @@ void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int 
                       float2* acc, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     float2* Y = P.work.as<float2>();
+    // nz volumes in, nz box spectra out; then those in, the group table once and the accumulator in and out
+    prof_bytes("ns_slab_r2c", nz * (4.0 * P.N + box_bytes(P, b)));
+    prof_bytes("ns_slab_accum_axis3", nz * box_bytes(P, b) + 0.5 * box_bytes(P, b) + 2 * box_bytes(P, b));
     SlabArgs a = slab_args(P, b, nz);
     a.spec = Y;
     a.spec_zstride = P.SP;

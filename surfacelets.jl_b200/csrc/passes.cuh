@@ -86,6 +86,7 @@ struct LoadHPair {
     const float2* src;
     ZMap zm;
     Lines g;
+    float wpair = 1.f;   // weight of the bins that are not self-conjugate (0.5: adjoint of the R2C)
     __device__ __forceinline__ void operator()(float2* tile, int npad, int n, int l0, int T, int z) const {
         const float2* s = src + zm.off(z);
         const int h = n / 2 + 1;
@@ -108,6 +109,9 @@ struct LoadHPair {
             if (selfc) {
                 a.y = 0.f;
                 b.y = 0.f;
+            } else {
+                a = c_scale(a, wpair);
+                b = c_scale(b, wpair);
             }
             tile[t * npad + k] = make_float2(a.x - b.y, a.y + b.x);
             if (!selfc) tile[t * npad + (n - k)] = make_float2(a.x + b.y, b.x - a.y);
@@ -149,6 +153,7 @@ struct StoreHalfPair {
     float2* dst;
     ZMap zm;
     Lines g;
+    float wpair = 1.f;   // weight of the bins that are not self-conjugate (2: adjoint of the C2R)
     __device__ __forceinline__ void operator()(const float2* tile, int npad, int n, int l0, int T, int z) const {
         float2* d = dst + zm.off(z);
         const int h = n / 2 + 1;
@@ -169,6 +174,10 @@ struct StoreHalfPair {
             // A = (Z[k] + conj(Z[-k]))/2 ; B = (Z[k] - conj(Z[-k]))/(2i)
             float2 A = make_float2(0.5f * (zk.x + zm_.x), 0.5f * (zk.y - zm_.y));
             float2 B = make_float2(0.5f * (zk.y + zm_.y), -0.5f * (zk.x - zm_.x));
+            if (k != 0 && 2 * k != n) {
+                A = c_scale(A, wpair);
+                B = c_scale(B, wpair);
+            }
             if (la < g.nlines) d[g.base(la) + (long long)k * g.si] = A;
             if (la + 1 < g.nlines) d[g.base(la + 1) + (long long)k * g.si] = B;
         }

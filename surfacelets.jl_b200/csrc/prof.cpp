@@ -22,6 +22,7 @@ struct Rec {
 std::mutex g_mu;
 bool g_on = false;
 std::vector<Rec> g_recs;
+std::map<std::string, double> g_bytes;
 
 }  // namespace
 
@@ -44,6 +45,12 @@ void prof_end(int token, cudaStream_t st) {
     if (token < (int)g_recs.size()) cudaEventRecord(g_recs[token].b, st);
 }
 
+void prof_bytes(const char* tag, double bytes) {
+    if (!g_on) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_bytes[tag] += bytes;
+}
+
 }  // namespace sfl
 
 extern "C" {
@@ -60,6 +67,16 @@ int sfl_profile_reset(void) {
         cudaEventDestroy(r.b);
     }
     sfl::g_recs.clear();
+    sfl::g_bytes.clear();
+    return SFL_OK;
+}
+
+int sfl_profile_bytes(const char* tag, double* bytes) {
+    std::lock_guard<std::mutex> lk(sfl::g_mu);
+    double b = 0;
+    for (auto& kv : sfl::g_bytes)
+        if (!tag || kv.first == tag) b += kv.second;
+    if (bytes) *bytes = b;
     return SFL_OK;
 }
 

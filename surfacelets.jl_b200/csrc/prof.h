@@ -11,5 +11,8 @@ bool prof_on();
 // Returns a token for prof_end (-1 when profiling is off).
 int prof_begin(const char* tag, cudaStream_t st);
 void prof_end(int token, cudaStream_t st);
+// Adds a launch's algorithmic bytes (inputs read once, outputs written once)
+// to its tag's total; no-op when profiling is off.
+void prof_bytes(const char* tag, double bytes);
 
 }  // namespace sfl

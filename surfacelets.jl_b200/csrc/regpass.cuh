@@ -66,6 +66,7 @@ struct RLoadHPair {
     ZMap zm;
     Lines g;
     int n;
+    float wpair = 1.f;   // weight of the bins that are not self-conjugate (0.5: adjoint of the R2C)
     struct Ctx {
         const float2* a;
         const float2* b;
@@ -86,6 +87,9 @@ struct RLoadHPair {
         if (k == 0 || 2 * k == n) {
             A.y = 0.f;
             B.y = 0.f;
+        } else {
+            A = c_scale(A, wpair);
+            B = c_scale(B, wpair);
         }
         return 2 * i <= n ? make_float2(A.x - B.y, A.y + B.x) : make_float2(A.x + B.y, B.x - A.y);
     }
@@ -161,6 +165,7 @@ struct RStoreHalfPair {
     ZMap zm;
     Lines g;
     int n;
+    float wpair = 1.f;   // weight of the bins that are not self-conjugate (2: adjoint of the C2R)
     struct Ctx {
         float2* a;
         float2* b;
@@ -179,8 +184,9 @@ struct RStoreHalfPair {
             float2 zk = Z[k];
             float2 zn = Z[k == 0 ? 0 : n - k];
             long long o = (long long)k * g.si;
-            if (c.a) c.a[o] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-            if (c.b) c.b[o] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+            const float w = (k == 0 || 2 * k == n) ? 1.f : wpair;
+            if (c.a) c.a[o] = c_scale(make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y)), w);
+            if (c.b) c.b[o] = c_scale(make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x)), w);
         }
     }
 };

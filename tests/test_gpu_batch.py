@@ -1,0 +1,70 @@
+"""Batches replayed as one CUDA graph (sfl_batch_*) against a loop of plain
+calls: the same kernels on the same data, so the outputs agree bit for bit,
+also after the inputs are refilled in place between runs (the batch workload
+of mixed sizes and scale counts)."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import gpu_available
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+MEMBERS = [
+    ("ns", (64, 64, 64), dict(scales=3, direction_levels=[2, 2, 3])),
+    ("ns", (96, 64, 128), dict(scales=2, direction_levels=[1, 3], bernstein_order=6)),
+    ("ns", (64, 96, 64), dict(scales=2, direction_levels=[2, 1])),
+    ("ns", (40, 36, 48), dict(scales=2, direction_levels=[1, 2], bernstein_order=6)),
+    ("surf", (48, 48, 48), dict(scales=2, direction_levels=[1, 2])),
+]
+
+
+def _members(sfl):
+    out = []
+    for kind, dims, kw in MEMBERS:
+        t = sfl.NSSurfacelet(**kw) if kind == "ns" else sfl.Surfacelet(**kw)
+        out.append(sfl.make_workspace(t, "float32", dims))
+    out.append(out[0])          # one workspace twice: its transforms keep their order
+    return out
+
+
+def _coef(sfl, ws):
+    return sfl.similar_coefficients(ws.transform, sfl.volume_like(ws.dims))
+
+
+def test_batch_analyze_and_synthesize_equal_plain_calls(sfl):
+    wss = _members(sfl)
+    rng = np.random.default_rng(11)
+    xs = [sfl.to_device(rng.standard_normal(ws.dims).astype(np.float32)) for ws in wss]
+    cs = [_coef(sfl, ws) for ws in wss]
+    b = sfl.Batch(wss, xs, cs, "analyze")
+    for rnd in range(2):
+        if rnd:
+            for x in xs:      # refill in place; the graph keeps the pointers
+                x.copy_(sfl.to_device(rng.standard_normal(tuple(x.shape)).astype(np.float32)))
+        b.run()
+        torch.cuda.synchronize()
+        for ws, x, c in zip(wss, xs, cs):
+            assert torch.equal(c, sfl.analyze(ws, x)), ws.dims
+    ys = [sfl.volume_like(ws.dims) for ws in wss]
+    bs = sfl.Batch(wss, cs, ys, "synthesize")
+    bs.run()
+    torch.cuda.synchronize()
+    for ws, c, y, x in zip(wss, cs, ys, xs):
+        assert torch.equal(y, sfl.synthesize(ws, c)), ws.dims
+        assert float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x)) <= 1e-5
+    b.close()
+    bs.close()
+
+
+def test_batch_argument_errors(sfl):
+    wss = _members(sfl)[:2]
+    xs = [sfl.volume_like(ws.dims) for ws in wss]
+    cs = [_coef(sfl, ws) for ws in wss]
+    with pytest.raises(sfl.ArgumentError):
+        sfl.Batch(wss, xs[:1], cs, "analyze")
+    with pytest.raises(sfl.ArgumentError):
+        sfl.Batch(wss, xs, cs, "transpose")
+    with pytest.raises(sfl.DimensionMismatch):
+        sfl.Batch(wss, xs[::-1], cs, "analyze")

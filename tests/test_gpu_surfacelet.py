@@ -118,3 +118,63 @@ def test_plane_wave_lands_in_its_hourglass(sfl):
         e = np.array([float((sfl.subband(t, c, i, (n, n, n)).double() ** 2).sum()) for i in range(2, 14)])
         assert (int(np.argmax(e))) // 4 + 1 == K
         assert e.max() / e[4 * K - 4:4 * K].sum() > 0.6
+
+
+ADJ_CASES = [CASES[0], CASES[1], CASES[2], CASES[3], CASES[5]]
+
+
+@pytest.mark.parametrize("dims,mode,J,L,bo", ADJ_CASES)
+def test_adjoints_against_the_oracle_forward(sfl, dims, mode, J, L, bo):
+    # <A x, c> = <x, A^T c> and <S c, x> = <c, S^T x>, with A and S the float64
+    # oracle and the transposes from the device.  c (x) is correlated with A x
+    # (S c) so that the products are large and the test is relative.
+    t = sfl.Surfacelet(scales=J, direction_levels=L, pyramid_ratio=mode, checkerboard_order=bo)
+    T = D.make_tables(D.SurfParams.make(scales=J, direction_levels=L, pyramid_ratio=mode, checkerboard_order=bo), dims)
+    ws = sfl.make_workspace(t, "float32", dims)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        x = rng.standard_normal(dims).astype(np.float32)
+        Ax = D.analyze(T, x.astype(np.float64))
+        c = (Ax + rng.standard_normal(Ax.shape)).astype(np.float32)
+        Atc = sfl.to_host(sfl.adjoint_analyze(ws, sfl.to_device(c), dims=dims)).astype(np.float64)
+        lhs, rhs = float(np.dot(Ax, c)), float(np.sum(x * Atc))
+        assert abs(lhs - rhs) <= 2e-5 * abs(lhs), (lhs, rhs)
+        cc = rng.standard_normal(Ax.shape).astype(np.float32)
+        Sc = D.synthesize(T, cc.astype(np.float64))
+        y = (Sc + rng.standard_normal(dims)).astype(np.float32)
+        Sty = sfl.adjoint_synthesize(ws, sfl.to_device(y)).cpu().numpy().astype(np.float64)
+        lhs, rhs = float(np.sum(Sc * y)), float(np.dot(cc, Sty))
+        assert abs(lhs - rhs) <= 2e-5 * abs(lhs), (lhs, rhs)
+
+
+def test_adjoints_at_128_mode_2_and_complex_linearity(sfl):
+    # the device transposes against the device transforms at the 128^3 workload,
+    # and complex data = real + i imag exactly
+    dims = (128, 128, 128)
+    t = sfl.Surfacelet(scales=3, direction_levels=[2, 2, 3], pyramid_ratio=2)
+    ws = sfl.make_workspace(t, "float32", dims)
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = sfl.volume_like(dims)
+    x.copy_(torch.randn(dims, generator=g, device="cuda"))
+    Ax = sfl.analyze(ws, x)
+    c = Ax + torch.randn(Ax.shape, generator=g, device="cuda")
+    lhs = float((Ax.double() * c.double()).sum())
+    rhs = float((x.double() * sfl.adjoint_analyze(ws, c, dims=dims).double()).sum())
+    assert abs(lhs - rhs) <= 2e-5 * abs(lhs)
+    Sc = sfl.synthesize(ws, c)
+    y = Sc + x
+    lhs = float((Sc.double() * y.double()).sum())
+    rhs = float((c.double() * sfl.adjoint_synthesize(ws, y).double()).sum())
+    assert abs(lhs - rhs) <= 2e-5 * abs(lhs)
+    dz = (48, 24, 36)
+    tz = sfl.Surfacelet(scales=2, direction_levels=[1, 2])
+    wz = sfl.make_workspace(tz, "complex64", dz)
+    wr = sfl.make_workspace(tz, "float32", dz)
+    rng = np.random.default_rng(9)
+    cr = rng.standard_normal(wz.ncoeffs).astype(np.float32)
+    ci = rng.standard_normal(wz.ncoeffs).astype(np.float32)
+    zc = sfl.to_host(sfl.adjoint_analyze(wz, torch.from_numpy((cr + 1j * ci).astype(np.complex64)).cuda(), dims=dz))
+    zr = sfl.to_host(sfl.adjoint_analyze(wr, torch.from_numpy(cr).cuda(), dims=dz))
+    zi = sfl.to_host(sfl.adjoint_analyze(wr, torch.from_numpy(ci).cuda(), dims=dz))
+    assert np.array_equal(zc.real, zr) and np.array_equal(zc.imag, zi)
