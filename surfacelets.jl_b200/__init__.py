@@ -8,6 +8,7 @@ reference's AbstractMultiscaleTransforms interface over it.  There is no CPU
 fallback: importing the package fails if the library is missing.
 """
 
+from .autograd import analyze_ad, as_colmajor, synthesize_ad  # noqa: F401
 from .batch import Batch  # noqa: F401
 from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateError, lib  # noqa: F401
 from .transforms import (  # noqa: F401

@@ -1,0 +1,87 @@
+"""Gradients through the transforms (torch autograd over the C ABI) for the
+compressed-sensing loss of the complex workload
+
+    L(c) = 0.5 || M o FFT3(synthesize(c)) - y ||^2 + lam sum sqrt(|c|^2 + eps^2)
+
+with M a seeded Bernoulli(0.25) sampling mask and y = M o FFT3(phantom):
+the device gradient is held against the float64 oracle gradient (itself
+pinned by central differences in test_oracle_gradients.py), and the same for
+the gradient through analyze, x -> L(analyze(x)).  At 128^3 the device
+gradient is checked by central differences of the device loss."""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import gpu_available
+from oracle import ns as N
+
+from cs_problem import EPS, LAM, analyze_c, analyze_t_c, make_problem, oracle_grad
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="needs a CUDA device")]
+
+
+def device_loss(sfl, ws, c, M, y):
+    x = sfl.synthesize_ad(ws, c)
+    r = M * torch.fft.fftn(x) - y
+    return 0.5 * (r.abs() ** 2).sum() + LAM * torch.sqrt(c.abs() ** 2 + EPS ** 2).sum()
+
+
+def test_gradients_match_the_float64_oracle(sfl):
+    dims = (32, 32, 32)
+    kw = dict(scales=3, direction_levels=[2, 2, 3])
+    T = N.make_tables(N.NSParams.make(**kw), dims)
+    ph, M, y, rng = make_problem(dims, 3)
+    c0 = analyze_c(T, ph)
+    c = c0 + 0.1 * (rng.standard_normal(c0.shape) + 1j * rng.standard_normal(c0.shape))
+    g = oracle_grad(T, c, M, y)
+    # the device gradient (float32) against the oracle's
+    ws = sfl.make_workspace(sfl.NSSurfacelet(**kw), "complex64", dims)
+    cd = sfl.to_device(c.astype(np.complex64)).requires_grad_(True)
+    L = device_loss(sfl, ws, cd, torch.from_numpy(M.astype(np.float32)).cuda(),
+                    torch.from_numpy(y.astype(np.complex64)).cuda())
+    L.backward()
+    gd = sfl.to_host(sfl.as_colmajor(cd.grad))
+    assert np.linalg.norm(gd - g) / np.linalg.norm(g) <= 1e-5
+    # through analyze: x -> L(analyze(x)), gradient A^T grad_c, away from the
+    # data (x = phantom + noise), so that the data term carries the gradient
+    x = (ph + 0.1 * (rng.standard_normal(dims) + 1j * rng.standard_normal(dims))).astype(np.complex64)
+    xd = sfl.to_device(x).requires_grad_(True)
+    ca = sfl.analyze_ad(ws, xd)
+    La = device_loss(sfl, ws, ca, torch.from_numpy(M.astype(np.float32)).cuda(),
+                     torch.from_numpy(y.astype(np.complex64)).cuda())
+    La.backward()
+    gx = analyze_t_c(T, oracle_grad(T, analyze_c(T, x.astype(np.complex128)), M, y))
+    gxd = sfl.to_host(sfl.as_colmajor(xd.grad))
+    assert np.linalg.norm(gxd - gx) / np.linalg.norm(gx) <= 1e-4
+
+
+def test_device_gradient_by_central_differences_at_128(sfl):
+    dims = (128, 128, 128)
+    ws = sfl.make_workspace(sfl.NSSurfacelet(scales=3, direction_levels=[2, 2, 3]), "complex64", dims)
+    ph, M, y, rng = make_problem(dims, 4)
+    Md = torch.from_numpy(M.astype(np.float32)).cuda()
+    yd = torch.from_numpy(y.astype(np.complex64)).cuda()
+    c0 = sfl.analyze(ws, sfl.to_device(ph.astype(np.complex64)))
+    g = torch.Generator(device="cuda").manual_seed(8)
+    c = (c0 + 0.1 * torch.randn(c0.shape, dtype=torch.complex64, generator=g, device="cuda")).detach()
+    c = sfl.as_colmajor(c).requires_grad_(True)
+    device_loss(sfl, ws, c, Md, yd).backward()
+    grad = c.grad.detach()
+
+    def loss64(cc):
+        x = sfl.synthesize(ws, sfl.as_colmajor(cc)).to(torch.complex128)
+        r = Md.double() * torch.fft.fftn(x) - yd.to(torch.complex128)
+        cd = cc.to(torch.complex128)
+        return float(0.5 * (r.abs() ** 2).sum() + LAM * torch.sqrt(cd.abs() ** 2 + EPS ** 2).sum())
+
+    # directions with a component along the gradient, so that the directional
+    # derivative stands well above the float32 rounding of the loss
+    h = 0.05
+    ghat = grad / torch.linalg.vector_norm(grad)
+    for _ in range(4):
+        d = torch.randn(c.shape, dtype=torch.complex64, generator=g, device="cuda")
+        d = ghat + 0.5 * d / torch.linalg.vector_norm(d)
+        fd = (loss64(c.detach() + h * d) - loss64(c.detach() - h * d)) / (2 * h)
+        an = float((grad.conj() * d).real.double().sum())
+        assert abs(fd - an) <= 2e-3 * abs(an), (fd, an)
