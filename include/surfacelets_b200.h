@@ -238,6 +238,16 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
 int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name,
                           int32_t index, double* out, int64_t* count);
 
+/* ── bfloat16 coefficients (NSSurfacelet, Float32 volumes) ─────────────────
+ * No counterpart in the reference.  c is (n1, n2, n3, S) bfloat16, column-
+ * major like the float32 coefficients; scales holds S float32 (device
+ * memory): subband s = scales[s-1] * c[..., s-1], each scale the power of two
+ * at or above the subband's largest magnitude.  Half the coefficient memory
+ * of float32 at bfloat16 accuracy (about 3 significant digits).  Slab and
+ * line pipelines only. */
+int sfl_ns_analyze_bf16(sfl_plan* plan, const void* x, void* c, float* scales, void* stream);
+int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, void* x, void* stream);
+
 /* ── Batches ─────────────────────────────────────────────────────────────
  * Many transforms as one CUDA graph: batch_create runs each (plan, input,
  * output) once eagerly, then captures the sequence (distinct plans on up to

@@ -13,7 +13,7 @@ from .batch import Batch  # noqa: F401
 from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateError, lib  # noqa: F401
 from .transforms import (  # noqa: F401
     NSSurfacelet, Surfacelet, Workspace, adjoint_analyze, adjoint_analyze_, adjoint_synthesize,
-    adjoint_synthesize_, analyze, analyze_, checkerboard_orders, make_workspace, nsubbands,
+    adjoint_synthesize_, analyze, analyze_, analyze_bf16, analyze_synthesize_stream, synthesize_bf16, checkerboard_orders, make_workspace, nsubbands,
     similar_coefficients, subband, subband_layout, subband_sizes, supports_streaming, surfacelet_redundancy,
     synthesize, synthesize_, to_device, to_host, volume_like,
 )

@@ -88,6 +88,8 @@ SIGNATURES = {
                                       C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "sfl_surf_design_table": (C.c_int, [C.POINTER(SurfParams), Dims, C.c_char_p, C.c_int32,
                                         C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "sfl_ns_analyze_bf16": (C.c_int, [P, P, P, P, P]),
+    "sfl_ns_synthesize_bf16": (C.c_int, [P, P, P, P, P]),
     "sfl_batch_create": (C.c_int, [C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.c_int32,
                                    C.POINTER(P)]),
     "sfl_batch_run": (C.c_int, [P, P]),

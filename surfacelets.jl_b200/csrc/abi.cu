@@ -496,9 +496,10 @@ int sfl_adjoint_synthesize(sfl_plan* plan, const void* x, void* c, void* stream)
     });
 }
 
-static sfl::NSPlan& ns_of(sfl_plan* plan) {
+static sfl::NSPlan& ns_of(sfl_plan* plan, const char* what = "streaming") {
     need(plan, "plan");
-    if (plan->impl.kind != SFL_KIND_NS) throw sfl::ArgError("streaming is supported by NSSurfacelet plans only");
+    if (plan->impl.kind != SFL_KIND_NS)
+        throw sfl::ArgError(std::string(what) + " is supported by NSSurfacelet plans only");
     return *plan->impl.ns;
 }
 
@@ -641,6 +642,34 @@ int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const
         }
         *count = (int64_t)tmp.size();
         if (out) std::memcpy(out, tmp.data(), sizeof(double) * tmp.size());
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_analyze_bf16(sfl_plan* plan, const void* x, void* c, float* scales, void* stream) {
+    return guarded([&] {
+        need(x, "x");
+        need(c, "c");
+        need(scales, "scales");
+        sfl::NSPlan& N = ns_of(plan, "bfloat16 coefficients");
+        if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+        check_aligned(x, plan->impl.dtype, "x");
+        if (reinterpret_cast<uintptr_t>(c) % 2 != 0) throw sfl::ArgError("c is not aligned to its element type");
+        on_device(plan, [&] { sfl::ns_analyze_bf16(N, static_cast<const float*>(x), c, scales, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, void* x, void* stream) {
+    return guarded([&] {
+        need(x, "x");
+        need(c, "c");
+        need(scales, "scales");
+        sfl::NSPlan& N = ns_of(plan, "bfloat16 coefficients");
+        if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+        check_aligned(x, plan->impl.dtype, "x");
+        if (reinterpret_cast<uintptr_t>(c) % 2 != 0) throw sfl::ArgError("c is not aligned to its element type");
+        on_device(plan, [&] { sfl::ns_synthesize_bf16(N, c, scales, static_cast<float*>(x), as_stream(stream)); });
         return SFL_OK;
     });
 }

@@ -495,15 +495,6 @@ void pass_c2c(NSPlan& P, const float2* src, float2* dst, long long zstride, int 
     launch_pass(ld, sto, f->sh, g.nlines, nz, inv, st, tag);
 }
 
-// The coefficient subbands of items [i0, ...): subband s at (s-1)*N*es.
-ZMap subband_map(NSPlan& P, int i0, int es) {
-    ZMap zc;
-    zc.items = P.items.as<NSItem>();
-    zc.item0 = i0;
-    zc.sub_stride = P.N * es;
-    return zc;
-}
-
 void rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
     pass_r2c(P, x, ZMap{}, es, X, 0, 1, st);
     pass_c2c(P, X, X, 0, 1, false, 1, st);
@@ -583,53 +574,97 @@ void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz,
 
 }  // namespace
 
+// ── item ranges: the building blocks of the slab and line pipelines ─────────
+
+long long ns_spec_elems(const NSPlan& P) { return P.slab ? P.SP : P.H; }
+
+void ns_forward_spectrum(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
+    if (P.slab)
+        ns_slab_rfft3(P, x, es, X, st);
+    else
+        rfft3(P, x, es, X, st);
+}
+
+int ns_next_chunk(const NSPlan& P, int i0) {
+    return P.slab ? ns_slab_chunk_end(P, i0) : std::min(P.S, i0 + P.group);
+}
+
+void ns_analyze_range(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
+                      cudaStream_t st) {
+    if (P.slab)
+        ns_slab_analyze_items(P, X, vol, vz, es, i0, nz, synth_masks, st);
+    else
+        analyze_items(P, X, vol, vz, es, i0, nz, synth_masks, st);
+}
+
+void ns_acc_clear(NSPlan& P, float2* acc, float2* comp, cudaStream_t st) {
+    cuda_check(cudaMemsetAsync(acc, 0, sizeof(float2) * ns_spec_elems(P), st), "cudaMemsetAsync(acc)");
+    if (!P.slab) cuda_check(cudaMemsetAsync(comp, 0, sizeof(float2) * P.H, st), "cudaMemsetAsync(comp)");
+}
+
+void ns_accumulate_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                         float2* acc, float2* comp, cudaStream_t st) {
+    if (P.slab)
+        ns_slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, st);
+    else
+        synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, comp, false, st);
+}
+
+void ns_inverse_spectrum(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) {
+    if (P.slab)
+        ns_slab_irfft3(P, A, x, es, st);
+    else
+        irfft3(P, A, x, es, st);
+}
+
+ZMap ns_subband_map(const NSPlan& P, int i0, int es) {
+    ZMap zc;
+    zc.items = P.items.as<NSItem>();
+    zc.item0 = i0;
+    zc.sub_stride = P.N * es;
+    return zc;
+}
+
 void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
-    if (P.slab) return ns_slab_analyze(P, x, c, st, synth_masks);
     if (P.plane) return ns_plane_analyze(P, x, c, st, synth_masks);
     const int es = P.nch;
+    float2* X = P.X.as<float2>();
     for (int ch = 0; ch < P.nch; ++ch) {
-        float2* X = P.X.as<float2>();
-        rfft3(P, reinterpret_cast<const float*>(x) + ch, es, X, st);
-        for (int i0 = 0; i0 < P.S; i0 += P.group) {
-            int nz = std::min(P.group, P.S - i0);
-            analyze_items(P, X, reinterpret_cast<float*>(c) + ch, subband_map(P, i0, es), es, i0, nz, synth_masks,
-                          st);
+        ns_forward_spectrum(P, reinterpret_cast<const float*>(x) + ch, es, X, st);
+        for (int i0 = 0, i1; i0 < P.S; i0 = i1) {
+            i1 = ns_next_chunk(P, i0);
+            ns_analyze_range(P, X, reinterpret_cast<float*>(c) + ch, ns_subband_map(P, i0, es), es, i0, i1 - i0,
+                             synth_masks, st);
         }
     }
 }
 
 void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
-    if (P.slab) return ns_slab_synthesize(P, c, x, st, analysis_masks);
     if (P.plane) return ns_plane_synthesize(P, c, x, st, analysis_masks);
     const int es = P.nch;
+    float2* A = P.acc.as<float2>();
+    float2* K = P.comp.as<float2>();
     for (int ch = 0; ch < P.nch; ++ch) {
-        float2* A = P.acc.as<float2>();
-        for (int i0 = 0; i0 < P.S; i0 += P.group) {
-            int nz = std::min(P.group, P.S - i0);
-            synth_items(P, reinterpret_cast<const float*>(c) + ch, subband_map(P, i0, es), es, i0, nz,
-                        analysis_masks, A, P.comp.as<float2>(), i0 == 0, st);
+        ns_acc_clear(P, A, K, st);
+        for (int i0 = 0, i1; i0 < P.S; i0 = i1) {
+            i1 = ns_next_chunk(P, i0);
+            ns_accumulate_range(P, reinterpret_cast<const float*>(c) + ch, ns_subband_map(P, i0, es), es, i0,
+                                i1 - i0, analysis_masks, A, K, st);
         }
-        irfft3(P, A, reinterpret_cast<float*>(x) + ch, es, st);
+        ns_inverse_spectrum(P, A, reinterpret_cast<float*>(x) + ch, es, st);
     }
 }
 
 // ── streaming ────────────────────────────────────────────────────────────────
 
 void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
-    if (P.slab) {
-        ns_slab_stream_analyze_begin(P, x, st);
-        P.stream_mode = 1;
-        P.stream_pos = 0;
-        return;
-    }
     if (P.plane) {
         ns_plane_stream_analyze_begin(P, x, st);
-        P.stream_mode = 1;
-        P.stream_pos = 0;
-        return;
+    } else {
+        for (int ch = 0; ch < P.nch; ++ch)
+            ns_forward_spectrum(P, reinterpret_cast<const float*>(x) + ch, P.nch,
+                                P.X.as<float2>() + ch * ns_spec_elems(P), st);
     }
-    for (int ch = 0; ch < P.nch; ++ch)
-        rfft3(P, reinterpret_cast<const float*>(x) + ch, P.nch, P.X.as<float2>() + ch * P.H, st);
     P.stream_mode = 1;
     P.stream_pos = 0;
 }
@@ -641,21 +676,13 @@ int ns_stream_analyze_next(NSPlan& P, void* band, int* index, cudaStream_t st) {
         return SFL_DONE;
     }
     const NSItem& it = P.items_host[P.stream_pos];
-    if (P.slab) {
-        ns_slab_stream_analyze_one(P, P.stream_pos, band, st);
-        *index = it.s;
-        P.stream_pos += 1;
-        return SFL_OK;
-    }
     if (P.plane) {
         ns_plane_stream_analyze_one(P, P.stream_pos, band, st);
-        *index = it.s;
-        P.stream_pos += 1;
-        return SFL_OK;
+    } else {
+        for (int ch = 0; ch < P.nch; ++ch)
+            ns_analyze_range(P, P.X.as<float2>() + ch * ns_spec_elems(P), reinterpret_cast<float*>(band) + ch, ZMap{},
+                             P.nch, P.stream_pos, 1, false, st);
     }
-    for (int ch = 0; ch < P.nch; ++ch)
-        analyze_items(P, P.X.as<float2>() + ch * P.H, reinterpret_cast<float*>(band) + ch, ZMap{}, P.nch,
-                      P.stream_pos, 1, false, st);
     *index = it.s;
     P.stream_pos += 1;
     return SFL_OK;
@@ -676,37 +703,31 @@ int ns_stream_synth_next_index(NSPlan& P, int* index) {
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
     if (P.stream_mode != 2) throw StateError("no streaming synthesis is open on this plan");
     if (P.stream_pos >= P.S) throw StateError("every subband has already been pushed");
-    if (P.slab) {
-        ns_slab_stream_synth_push(P, P.stream_pos, band, st);
-        P.stream_pos += 1;
-        return;
-    }
     if (P.plane) {
         ns_plane_stream_synth_push(P, P.stream_pos, band, st);
-        P.stream_pos += 1;
-        return;
+    } else {
+        const long long E = ns_spec_elems(P);
+        for (int ch = 0; ch < P.nch; ++ch) {
+            float2* A = P.acc.as<float2>() + ch * E;
+            float2* K = P.comp.as<float2>() + ch * P.H;
+            if (P.stream_pos == 0) ns_acc_clear(P, A, K, st);
+            ns_accumulate_range(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1, false,
+                                A, K, st);
+        }
     }
-    for (int ch = 0; ch < P.nch; ++ch)
-        synth_items(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1, false,
-                    P.acc.as<float2>() + ch * P.H, P.comp.as<float2>() + ch * P.H, P.stream_pos == 0, st);
     P.stream_pos += 1;
 }
 
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
     if (P.stream_mode != 2 || P.stream_pos != P.S)
         throw StateError("streaming synthesis ended before every subband was pushed");
-    if (P.slab) {
-        ns_slab_stream_synth_end(P, x, st);
-        P.stream_mode = 0;
-        return;
-    }
     if (P.plane) {
         ns_plane_stream_synth_end(P, x, st);
-        P.stream_mode = 0;
-        return;
+    } else {
+        for (int ch = 0; ch < P.nch; ++ch)
+            ns_inverse_spectrum(P, P.acc.as<float2>() + ch * ns_spec_elems(P), reinterpret_cast<float*>(x) + ch, P.nch,
+                                st);
     }
-    for (int ch = 0; ch < P.nch; ++ch)
-        irfft3(P, P.acc.as<float2>() + ch * P.H, reinterpret_cast<float*>(x) + ch, P.nch, st);
     P.stream_mode = 0;
 }
 

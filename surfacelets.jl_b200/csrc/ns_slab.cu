@@ -682,14 +682,6 @@ int chunk_end(const NSPlan& P, int i0) {
     return i1;
 }
 
-ZMap subband_zmap(const NSPlan& P, int i0, int es) {
-    ZMap zc;
-    zc.items = P.items.as<NSItem>();
-    zc.item0 = i0;
-    zc.sub_stride = P.N * es;
-    return zc;
-}
-
 }  // namespace
 
 bool ns_slab_supported(int n1, int n2, int n3) {
@@ -734,57 +726,20 @@ void ns_use_slabs(NSPlan& P) {
     ns_alloc_scratch(P);
 }
 
-void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
-    const int es = P.nch;
-    float2* X = P.X.as<float2>();
-    for (int ch = 0; ch < P.nch; ++ch) {
-        slab_rfft3(P, reinterpret_cast<const float*>(x) + ch, es, X, st);
-        for (int i0 = 0; i0 < P.S;) {
-            const int i1 = chunk_end(P, i0);
-            slab_analyze_items(P, X, reinterpret_cast<float*>(c) + ch, subband_zmap(P, i0, es), es, i0, i1 - i0,
-                               synth_masks, st);
-            i0 = i1;
-        }
-    }
+void ns_slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) { slab_rfft3(P, x, es, X, st); }
+
+void ns_slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) { slab_irfft3(P, A, x, es, st); }
+
+int ns_slab_chunk_end(const NSPlan& P, int i0) { return chunk_end(P, i0); }
+
+void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
+                           cudaStream_t st) {
+    slab_analyze_items(P, X, vol, vz, es, i0, nz, synth_masks, st);
 }
 
-void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
-    const int es = P.nch;
-    float2* A = P.acc.as<float2>();
-    for (int ch = 0; ch < P.nch; ++ch) {
-        cuda_check(cudaMemsetAsync(A, 0, sizeof(float2) * P.SP, st), "cudaMemsetAsync(acc)");
-        for (int i0 = 0; i0 < P.S;) {
-            const int i1 = chunk_end(P, i0);
-            slab_synth_items(P, reinterpret_cast<const float*>(c) + ch, subband_zmap(P, i0, es), es, i0, i1 - i0,
-                             analysis_masks, A, st);
-            i0 = i1;
-        }
-        slab_irfft3(P, A, reinterpret_cast<float*>(x) + ch, es, st);
-    }
-}
-
-void ns_slab_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
-    for (int ch = 0; ch < P.nch; ++ch)
-        slab_rfft3(P, reinterpret_cast<const float*>(x) + ch, P.nch, P.X.as<float2>() + ch * P.SP, st);
-}
-
-void ns_slab_stream_analyze_one(NSPlan& P, int pos, void* band, cudaStream_t st) {
-    for (int ch = 0; ch < P.nch; ++ch)
-        slab_analyze_items(P, P.X.as<float2>() + ch * P.SP, reinterpret_cast<float*>(band) + ch, ZMap{}, P.nch, pos,
-                           1, false, st);
-}
-
-void ns_slab_stream_synth_push(NSPlan& P, int pos, const void* band, cudaStream_t st) {
-    if (pos == 0)
-        cuda_check(cudaMemsetAsync(P.acc.p, 0, sizeof(float2) * P.SP * P.nch, st), "cudaMemsetAsync(acc)");
-    for (int ch = 0; ch < P.nch; ++ch)
-        slab_synth_items(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, pos, 1, false,
-                         P.acc.as<float2>() + ch * P.SP, st);
-}
-
-void ns_slab_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
-    for (int ch = 0; ch < P.nch; ++ch)
-        slab_irfft3(P, P.acc.as<float2>() + ch * P.SP, reinterpret_cast<float*>(x) + ch, P.nch, st);
+void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                         float2* acc, cudaStream_t st) {
+    slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, st);
 }
 
 }  // namespace sfl

@@ -9,18 +9,6 @@
 
 namespace sfl {
 
-// Where item z of a batched launch starts: a fixed stride, or the subband
-// named by an NS item (offset (s-1)*sub_stride).
-struct ZMap {
-    const NSItem* items = nullptr;
-    int item0 = 0;
-    long long sub_stride = 0;
-    long long zstride = 0;
-    __device__ __forceinline__ long long off(int z) const {
-        return items ? (long long)(items[item0 + z].s - 1) * sub_stride : (long long)z * zstride;
-    }
-};
-
 // ── loads ────────────────────────────────────────────────────────────────────
 
 // Complex lines, optionally scaled.

@@ -65,6 +65,18 @@ struct NSItem {
     int wb_lo, wb_hi, wb_dlo;
 };
 
+// Where item z of a batched launch starts: a fixed stride, or the subband
+// named by an NS item (offset (s-1)*sub_stride).
+struct ZMap {
+    const NSItem* items = nullptr;
+    int item0 = 0;
+    long long sub_stride = 0;
+    long long zstride = 0;
+    __device__ __forceinline__ long long off(int z) const {
+        return items ? (long long)(items[item0 + z].s - 1) * sub_stride : (long long)z * zstride;
+    }
+};
+
 // Mask tables on the device: the group masks (float64-designed, one rfft
 // grid each), the level bandpasses (synthesis of a bank that is not tight),
 // the lowpass's per-axis factors and the wedge planes.
@@ -114,6 +126,7 @@ struct NSPlan {
     DevMem X;        // nch spectra
     DevMem work;     // group spectra
     DevMem acc, comp;   // nch accumulators (+ Kahan compensation)
+    DevMem band, maxbits;   // float32 subbands of a chunk and their peaks (bfloat16 coefficients)
     // streaming state
     int stream_mode = 0;    // 0 idle, 1 analyzing, 2 synthesizing
     int stream_pos = 0;
@@ -156,12 +169,30 @@ void ns_use_slabs(NSPlan& P);
 NSBox ns_make_box(int nk1, int b2, int n2);
 NSBox ns_table_box(const std::vector<double>& g, int h1, int n2, int n3);
 void ns_alloc_scratch(NSPlan& P);
-void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
-void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
-void ns_slab_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);
-void ns_slab_stream_analyze_one(NSPlan& P, int pos, void* band, cudaStream_t st);
-void ns_slab_stream_synth_push(NSPlan& P, int pos, const void* band, cudaStream_t st);
-void ns_slab_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
+void ns_slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st);
+void ns_slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st);
+int ns_slab_chunk_end(const NSPlan& P, int i0);
+void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
+                           cudaStream_t st);
+void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                         float2* acc, cudaStream_t st);
+// Item-range building blocks of the slab and line pipelines (ns.cu): the
+// spectrum of a channel, the launch chunks, the analysis of items into
+// volumes at vol + vz.off(z), their accumulation into a spectrum, and its
+// inverse.  Spectra hold ns_spec_elems bins.
+long long ns_spec_elems(const NSPlan& P);
+void ns_forward_spectrum(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st);
+int ns_next_chunk(const NSPlan& P, int i0);
+void ns_analyze_range(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
+                      cudaStream_t st);
+void ns_acc_clear(NSPlan& P, float2* acc, float2* comp, cudaStream_t st);
+void ns_accumulate_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                         float2* acc, float2* comp, cudaStream_t st);
+void ns_inverse_spectrum(NSPlan& P, float2* A, float* x, int es, cudaStream_t st);
+ZMap ns_subband_map(const NSPlan& P, int i0, int es);
+// bfloat16 coefficients with a float32 scale per subband (ns_bf16.cu).
+void ns_analyze_bf16(NSPlan& P, const float* x, void* c, float* scales, cudaStream_t st);
+void ns_synthesize_bf16(NSPlan& P, const void* c, const float* scales, float* x, cudaStream_t st);
 void ns_plane_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
 void ns_plane_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
 void ns_plane_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);

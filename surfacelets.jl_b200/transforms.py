@@ -249,7 +249,8 @@ def _need_torch():
 def volume_like(dims, dtype="float32", device="cuda"):
     """Uninitialized column-major device array of shape dims (torch)."""
     _need_torch()
-    td = torch.complex64 if str(dtype) in ("complex64", "torch.complex64") else torch.float32
+    td = {"complex64": torch.complex64, "torch.complex64": torch.complex64, "bfloat16": torch.bfloat16,
+          "torch.bfloat16": torch.bfloat16}.get(str(dtype), torch.float32)
     return torch.empty(tuple(reversed(tuple(dims))), dtype=td, device=device).permute(*reversed(range(len(dims))))
 
 
@@ -635,3 +636,74 @@ def _synthesize_stream(f, x, t, workspace, stream):
     if host:
         _copy_back(x, xd)
     return x
+
+
+# ── bfloat16 coefficients ───────────────────────────────────────────────────
+
+
+def analyze_bf16(ws, x, stream=None):
+    """NSSurfacelet analysis into bfloat16 coefficients: returns (c, scales)
+    with c (n1, n2, n3, S) bfloat16 and scales (S,) float32 on the device,
+    subband s = scales[s-1] * c[..., s-1] (each scale a power of two, the
+    stored values within [-1, 1]).  Float32 volumes; no counterpart in the
+    reference."""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NSSurfacelet):
+        raise ArgumentError("bfloat16 coefficients need an NSSurfacelet workspace")
+    _check_device_array(x, "volume", ws.dims, ws.dtype)
+    c = volume_like(ws.dims + (ws.nsubbands,), "bfloat16", x.device)
+    scales = torch.empty(ws.nsubbands, dtype=torch.float32, device=x.device)
+    check(lib.sfl_ns_analyze_bf16(ws._h, _ptr(x), _ptr(c), _ptr(scales), _stream(stream)))
+    return c, scales
+
+
+def synthesize_bf16(ws, c, scales, stream=None):
+    """Synthesis from analyze_bf16's (c, scales)."""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NSSurfacelet):
+        raise ArgumentError("bfloat16 coefficients need an NSSurfacelet workspace")
+    shape = ws.dims + (ws.nsubbands,)
+    if tuple(c.shape) != shape:
+        raise DimensionMismatch(f"coefficients of size {tuple(c.shape)}, expected {shape}")
+    if c.dtype != torch.bfloat16 or not c.is_cuda or not _is_colmajor(c):
+        raise ArgumentError("coefficients must be a column-major bfloat16 CUDA tensor")
+    if tuple(scales.shape) != (ws.nsubbands,) or scales.dtype != torch.float32 or not scales.is_cuda:
+        raise ArgumentError(f"scales must be {ws.nsubbands} float32 values on the device")
+    x = volume_like(ws.dims, "float32", c.device)
+    check(lib.sfl_ns_synthesize_bf16(ws._h, _ptr(c), _ptr(scales), _ptr(x), _stream(stream)))
+    return x
+
+
+# ── analysis -> per-subband processing -> synthesis, one subband at a time ──
+
+
+def analyze_synthesize_stream(f, y, x, analysis_workspace, synthesis_workspace, stream=None):
+    """y = sum_i S_i f(i, A_i x): subband i of x, handed to f(i, band) on the
+    device, goes straight into the synthesis, so only one subband is ever in
+    memory (a per-subband recompute instead of a materialized coefficient
+    set; f = a shrinkage gives a denoiser).  The two workspaces are two plans
+    of the same NSSurfacelet, size and element type (one per direction).
+    f may modify band in place and return it, or return a new tensor; it runs
+    on the current stream.  Built from the reference's streaming analyze(f, t,
+    x) and synthesize!(f, x, t), src/transforms/ns_surfacelet.jl:600-641."""
+    wa, wsy = analysis_workspace, synthesis_workspace
+    for w in (wa, wsy):
+        if not isinstance(w, Workspace) or not isinstance(w.transform, NSSurfacelet):
+            raise ArgumentError("analyze_synthesize_stream needs two NSSurfacelet workspaces")
+    if wa is wsy or wa._h.value == wsy._h.value:
+        raise ArgumentError("analysis and synthesis need two workspaces (a plan holds one open stream)")
+    if (wa.dims, wa.dtype, wa.nsubbands) != (wsy.dims, wsy.dtype, wsy.nsubbands):
+        raise ArgumentError("the two workspaces must match in size, element type and subbands")
+    _check_device_array(x, "volume", wa.dims, wa.dtype)
+    _check_device_array(y, "output volume", wa.dims, wa.dtype)
+    st = _stream(stream)
+    band = volume_like(wa.dims, "complex64" if wa.dtype else "float32", x.device)
+    check(lib.sfl_stream_analyze_begin(wa._h, _ptr(x), st))
+    check(lib.sfl_stream_synthesize_begin(wsy._h, st))
+    i, j = C.c_int32(), C.c_int32()
+    while check(lib.sfl_stream_analyze_next(wa._h, _ptr(band), C.byref(i), st)) != _lib.SFL_DONE:
+        check(lib.sfl_stream_synthesize_next_index(wsy._h, C.byref(j)))
+        out = f(i.value, band)
+        out = band if out is None else out
+        _check_device_array(out, f"processed subband {i.value}", wa.dims, wa.dtype)
+        check(lib.sfl_stream_synthesize_push(wsy._h, _ptr(out), st))
+    check(lib.sfl_stream_synthesize_end(wsy._h, _ptr(y), st))
+    return y
