@@ -238,6 +238,27 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
 int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name,
                           int32_t index, double* out, int64_t* count);
 
+/* ── Item ranges (NSSurfacelet; sharding subbands across devices) ────────
+ * No counterpart in the reference.  The subbands in stream order (stream_order
+ * gives the subband index at each of the S positions) split into ranges:
+ *   forward_spectrum   X = the spectrum of x, nch x spectrum_elems complex
+ *                      float32 bins in the plan's internal layout (opaque);
+ *   analyze_range      the subbands at positions [first, first + count) from
+ *                      X into count consecutive volumes of c;
+ *   accumulate_range   their synthesis contributions into the spectrum A
+ *                      (clear != 0 zeroes A first);
+ *   inverse_spectrum   x from an accumulated spectrum (A is overwritten).
+ * Accumulated spectra add: the sum over devices of each device's
+ * accumulation of its own ranges is the accumulation of all of them.  Slab
+ * and line pipelines only; not while a stream is open. */
+int sfl_ns_spectrum_elems(const sfl_plan* plan, int64_t* elems);
+int sfl_ns_stream_order(const sfl_plan* plan, int32_t* subband_index);
+int sfl_ns_forward_spectrum(sfl_plan* plan, const void* x, void* X, void* stream);
+int sfl_ns_analyze_range(sfl_plan* plan, const void* X, int32_t first, int32_t count, void* c, void* stream);
+int sfl_ns_accumulate_range(sfl_plan* plan, const void* c, int32_t first, int32_t count, void* A, int32_t clear,
+                            void* stream);
+int sfl_ns_inverse_spectrum(sfl_plan* plan, void* A, void* x, void* stream);
+
 /* ── bfloat16 coefficients (NSSurfacelet, Float32 volumes) ─────────────────
  * No counterpart in the reference.  c is (n1, n2, n3, S) bfloat16, column-
  * major like the float32 coefficients; scales holds S float32 (device

@@ -10,6 +10,7 @@ fallback: importing the package fails if the library is missing.
 
 from .autograd import analyze_ad, as_colmajor, synthesize_ad  # noqa: F401
 from .batch import Batch  # noqa: F401
+from .sharded import LibRanges, analyze_sharded, shard, synthesize_sharded  # noqa: F401
 from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateError, lib  # noqa: F401
 from .transforms import (  # noqa: F401
     NSSurfacelet, Surfacelet, Workspace, adjoint_analyze, adjoint_analyze_, adjoint_synthesize,

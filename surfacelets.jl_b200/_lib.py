@@ -88,6 +88,12 @@ SIGNATURES = {
                                       C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "sfl_surf_design_table": (C.c_int, [C.POINTER(SurfParams), Dims, C.c_char_p, C.c_int32,
                                         C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "sfl_ns_spectrum_elems": (C.c_int, [P, C.POINTER(C.c_int64)]),
+    "sfl_ns_stream_order": (C.c_int, [P, C.POINTER(C.c_int32)]),
+    "sfl_ns_forward_spectrum": (C.c_int, [P, P, P, P]),
+    "sfl_ns_analyze_range": (C.c_int, [P, P, C.c_int32, C.c_int32, P, P]),
+    "sfl_ns_accumulate_range": (C.c_int, [P, P, C.c_int32, C.c_int32, P, C.c_int32, P]),
+    "sfl_ns_inverse_spectrum": (C.c_int, [P, P, P, P]),
     "sfl_ns_analyze_bf16": (C.c_int, [P, P, P, P, P]),
     "sfl_ns_synthesize_bf16": (C.c_int, [P, P, P, P, P]),
     "sfl_batch_create": (C.c_int, [C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.c_int32,

@@ -674,6 +674,124 @@ int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, v
     });
 }
 
+// ── item ranges (sharding subbands across devices) ──────────────────────────
+
+static sfl::NSPlan& range_plan(sfl_plan* plan) {
+    sfl::NSPlan& N = ns_of(plan, "item ranges");
+    if (N.plane) throw sfl::ArgError("item ranges need the slab or line pipeline");
+    if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+    return N;
+}
+
+static void check_range(const sfl::NSPlan& N, int32_t first, int32_t count) {
+    if (first < 0 || count < 0 || first + count > N.S)
+        throw sfl::ArgError("stream positions [" + std::to_string(first) + ", " + std::to_string(first + count) +
+                            ") are outside [0, " + std::to_string(N.S) + ")");
+}
+
+int sfl_ns_spectrum_elems(const sfl_plan* plan, int64_t* elems) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(elems, "elems");
+        if (plan->impl.kind != SFL_KIND_NS) throw sfl::ArgError("item ranges are supported by NSSurfacelet plans only");
+        *elems = sfl::ns_spec_elems(*plan->impl.ns);
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_stream_order(const sfl_plan* plan, int32_t* subband_index) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(subband_index, "subband_index");
+        if (plan->impl.kind != SFL_KIND_NS) throw sfl::ArgError("item ranges are supported by NSSurfacelet plans only");
+        const sfl::NSPlan& N = *plan->impl.ns;
+        for (int i = 0; i < N.S; ++i) subband_index[i] = N.items_host[i].s;
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_forward_spectrum(sfl_plan* plan, const void* x, void* X, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = range_plan(plan);
+        need(x, "x");
+        need(X, "X");
+        check_aligned(x, plan->impl.dtype, "x");
+        const long long E = sfl::ns_spec_elems(N);
+        on_device(plan, [&] {
+            for (int ch = 0; ch < N.nch; ++ch)
+                sfl::ns_forward_spectrum(N, static_cast<const float*>(x) + ch, N.nch, static_cast<float2*>(X) + ch * E,
+                                         as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_analyze_range(sfl_plan* plan, const void* X, int32_t first, int32_t count, void* c, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = range_plan(plan);
+        need(X, "X");
+        need(c, "c");
+        check_aligned(c, plan->impl.dtype, "c");
+        check_range(N, first, count);
+        const long long E = sfl::ns_spec_elems(N);
+        on_device(plan, [&] {
+            for (int ch = 0; ch < N.nch; ++ch)
+                for (int i0 = first, i1; i0 < first + count; i0 = i1) {
+                    i1 = std::min(sfl::ns_next_chunk(N, i0), first + count);
+                    sfl::ZMap vz;
+                    vz.zstride = N.N * N.nch;
+                    float* base = static_cast<float*>(c) + (long long)(i0 - first) * N.N * N.nch + ch;
+                    sfl::ns_analyze_range(N, static_cast<const float2*>(X) + ch * E, base, vz, N.nch, i0, i1 - i0,
+                                          false, as_stream(stream));
+                }
+        });
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_accumulate_range(sfl_plan* plan, const void* c, int32_t first, int32_t count, void* A, int32_t clear,
+                            void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = range_plan(plan);
+        need(c, "c");
+        need(A, "A");
+        check_aligned(c, plan->impl.dtype, "c");
+        check_range(N, first, count);
+        const long long E = sfl::ns_spec_elems(N);
+        on_device(plan, [&] {
+            for (int ch = 0; ch < N.nch; ++ch) {
+                float2* acc = static_cast<float2*>(A) + ch * E;
+                float2* comp = N.comp.as<float2>() + (N.slab ? 0 : ch * N.H);
+                if (clear) sfl::ns_acc_clear(N, acc, comp, as_stream(stream));
+                for (int i0 = first, i1; i0 < first + count; i0 = i1) {
+                    i1 = std::min(sfl::ns_next_chunk(N, i0), first + count);
+                    sfl::ZMap vz;
+                    vz.zstride = N.N * N.nch;
+                    const float* base = static_cast<const float*>(c) + (long long)(i0 - first) * N.N * N.nch + ch;
+                    sfl::ns_accumulate_range(N, base, vz, N.nch, i0, i1 - i0, false, acc, comp, as_stream(stream));
+                }
+            }
+        });
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_inverse_spectrum(sfl_plan* plan, void* A, void* x, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = range_plan(plan);
+        need(A, "A");
+        need(x, "x");
+        check_aligned(x, plan->impl.dtype, "x");
+        const long long E = sfl::ns_spec_elems(N);
+        on_device(plan, [&] {
+            for (int ch = 0; ch < N.nch; ++ch)
+                sfl::ns_inverse_spectrum(N, static_cast<float2*>(A) + ch * E, static_cast<float*>(x) + ch, N.nch,
+                                         as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
 // ── batches: one CUDA graph over many transforms ─────────────────────────────
 
 int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* inputs, void* const* outputs,

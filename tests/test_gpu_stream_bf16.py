@@ -16,7 +16,8 @@ pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not gpu_available(), reason="n
 
 
 def rel(a, b):
-    return float(torch.linalg.vector_norm((a - b).double()) / torch.linalg.vector_norm(b.double()))
+    d = torch.complex128 if a.is_complex() or b.is_complex() else torch.float64
+    return float(torch.linalg.vector_norm((a - b).to(d)) / torch.linalg.vector_norm(b.to(d)))
 
 
 def soft(b, tau):
