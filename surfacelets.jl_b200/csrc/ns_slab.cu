@@ -204,13 +204,19 @@ __device__ __forceinline__ void load_slab_twiddles(float2* tw2, const float2* __
     }
 }
 
+// Axis-1 pitch of a padded spectrum with h1 bins on axis 1: the smallest
+// P1 >= h1 with P1 = 2 mod 4.
+constexpr int slab_pitch_c(int h1) { return h1 % 4 == 2 ? h1 : slab_pitch_c(h1 + 1); }
+
 // FFT of one line of N points held by the N2 lanes p of a warp: v[r] holds
 // x[p + N2 r] on entry and X[(p + N2 j) + N1 k] at v[j N2 + k] on exit.  The
-// exchange runs through slot(t), t < N, which only this line touches; lanes
-// of invalid lines skip every slot access but keep to the warp barriers.
-template <int N, bool INV, class Slot>
+// exchange runs through the line's own slots base[STRIDE t], t < N, with
+// slot (sender q, value m) at t = N2 m + (q ^ (m mod N2)): conflict-free
+// writes and reads for STRIDE = 1 and for STRIDE = 2 mod 4.  Lanes of
+// invalid lines skip every slot access but keep to the warp barriers.
+template <int N, bool INV, int STRIDE>
 __device__ __forceinline__ void warp_line_fft(float2 (&v)[LinePlan<N>::N1], int p, bool valid,
-                                              const float2* __restrict__ tw2, const Slot& slot) {
+                                              const float2* __restrict__ tw2, float2* base) {
     using L = SlabLine<N>;
     constexpr int N1 = L::N1, N2 = L::N2;
     RegDft<N1, INV>::run(v);
@@ -220,18 +226,23 @@ __device__ __forceinline__ void warp_line_fft(float2 (&v)[LinePlan<N>::N1], int 
         if (INV) w.y = -w.y;
         v[m] = c_mul(v[m], w);
     }
+    // x[c] = STRIDE (p ^ c): the sender-dependent part of a slot, shared by both sides
+    int xo[N2];
+#pragma unroll
+    for (int c = 0; c < N2; ++c) xo[c] = STRIDE * (p ^ c);
     __syncwarp();   // the line's inputs may have come from its own slots
     if (valid) {
 #pragma unroll
-        for (int m = 0; m < N1; ++m) *slot(m * N2 + (p ^ (m & (N2 - 1)))) = v[m];
+        for (int m = 0; m < N1; ++m) base[xo[m & (N2 - 1)] + STRIDE * N2 * m] = v[m];
     }
     __syncwarp();
+    const float2* rb = base + STRIDE * N2 * p;
 #pragma unroll
     for (int j = 0; j < L::M; ++j) {
-        const int m = p + N2 * j;
         float2 w[N2];
 #pragma unroll
-        for (int pp = 0; pp < N2; ++pp) w[pp] = valid ? *slot(m * N2 + (pp ^ p)) : make_float2(0.f, 0.f);
+        for (int pp = 0; pp < N2; ++pp)
+            w[pp] = valid ? rb[xo[pp] + STRIDE * N2 * N2 * j] : make_float2(0.f, 0.f);
         RegDft<N2, INV>::run(w);
 #pragma unroll
         for (int k = 0; k < N2; ++k) v[j * N2 + k] = w[k];
@@ -248,29 +259,16 @@ __device__ __forceinline__ int pair_subline(int s) {
     return s;
 }
 
-struct RowSlot {
-    float2* base;
-    int P1;
-    __device__ __forceinline__ float2* operator()(int t) const { return base + P1 * t; }
-};
-
-struct PairSlot {
-    float2* a;
-    float2* b;
-    int split;
-    __device__ __forceinline__ float2* operator()(int t) const { return t < split ? a + t : b + (t - split); }
-};
-
-template <int NA, int NB>
-struct SlabSmem {
-    static size_t bytes(int P1) { return sizeof(float2) * ((size_t)NA + NB + (size_t)P1 * NB); }
-};
-
-// Analysis slab pass (inverse): spectra -> real volumes.
-template <int NA, int NB, int MINB>
+// Analysis slab pass (inverse): spectra -> real volumes (element stride ES).
+// The exchange slots of a column pair are the pair's two columns read as one
+// run of 2 P1 >= NA values.
+template <int NA, int NB, int ES, int MINB>
 __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArgs a) {
     using LA = SlabLine<NA>;
     using LB = SlabLine<NB>;
+    constexpr int P1 = slab_pitch_c(NA / 2 + 1);
+    constexpr int SL = P1 * NB;
+    constexpr long long PLANE = (long long)NA * NB;
     extern __shared__ float2 sm[];
     float2* twA = sm;
     float2* twB = sm + NA;
@@ -278,34 +276,33 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
     load_slab_twiddles<NA>(twA, a.twa);
     load_slab_twiddles<NB>(twB, a.twb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int P1 = a.P1;
-    const int SL = P1 * NB;
-    const long long plane = (long long)NA * NB;
+    const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
+    const int k2hi = NB - (nk2 - b2 - 1);   // first negative-frequency column in the box
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
         const int z = u / a.n3, s3 = u - z * a.n3;
         const float2* src = a.spec + z * a.spec_zstride + (long long)s3 * SL;
         // 1. the box of the slab into shared memory
-        for (int j = warp; j < a.nk2; j += kSlabWarps) {
-            const int k2 = j <= a.b2 ? j : j + (NB - a.nk2);
-            for (int k1 = lane; k1 < a.nk1; k1 += 32) S[k1 + P1 * k2] = src[k1 + P1 * k2];
+        for (int j = warp; j < nk2; j += kSlabWarps) {
+            const int k2 = j <= b2 ? j : j + (NB - nk2);
+            for (int k1 = lane; k1 < nk1; k1 += 32) S[k1 + P1 * k2] = src[k1 + P1 * k2];
         }
         __syncthreads();
         // 2. inverse FFT along axis 2 of the rows k1 < nk1; columns outside the box are zero
         {
-            const int p = lane % LB::N2, s = lane / LB::N2;
-            for (int base = 0; base < a.nk1; base += LB::LPR) {
-                if (base + warp * LB::LPW >= a.nk1) continue;   // warp-uniform
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
                 const int k1 = base + warp * LB::LPW + s;
-                const bool valid = k1 < a.nk1;
+                const bool valid = k1 < nk1;
                 float2* row = S + (valid ? k1 : 0);
                 float2 v[LB::N1];
 #pragma unroll
                 for (int r = 0; r < LB::N1; ++r) {
                     const int k2 = p + LB::N2 * r;
-                    const bool in = valid && (k2 <= a.b2 || k2 >= NB - (a.nk2 - a.b2 - 1));
+                    const bool in = valid && (k2 <= b2 || k2 >= k2hi);
                     v[r] = in ? row[P1 * k2] : make_float2(0.f, 0.f);
                 }
-                warp_line_fft<NB, true>(v, p, valid, twB, RowSlot{row, P1});
+                warp_line_fft<NB, true, P1>(v, p, valid, twB, row);
                 if (valid) {
 #pragma unroll
                     for (int j = 0; j < LB::M; ++j)
@@ -317,9 +314,9 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
         __syncthreads();
         // 3. C2R along axis 1, columns 2l and 2l+1 as one complex line; rows k1 >= nk1 are zero
         {
-            const int p = lane % LA::N2, s = pair_subline<NA>(lane / LA::N2);
+            const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
             constexpr int npairs = NB / 2;
-            float* out = a.vol + a.vz.off(z) + (long long)s3 * plane * a.es;
+            float* out = a.vol + a.vz.off(z) + (long long)s3 * PLANE * ES;
             for (int base = 0; base < npairs; base += LA::LPR) {
                 if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
                 const int l = base + warp * LA::LPW + s;
@@ -332,7 +329,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
                     const int i = p + LA::N2 * r;
                     const int k = 2 * i <= NA ? i : NA - i;
                     float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
-                    if (valid && k < a.nk1) {
+                    if (valid && k < nk1) {
                         A = ca[k];
                         B = cb[k];
                     }
@@ -342,17 +339,18 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
                     }
                     v[r] = 2 * i <= NA ? make_float2(A.x - B.y, A.y + B.x) : make_float2(A.x + B.y, B.x - A.y);
                 }
-                warp_line_fft<NA, true>(v, p, valid, twA, PairSlot{ca, cb, (NA + 1) / 2});
+                warp_line_fft<NA, true, 1>(v, p, valid, twA, ca);
                 if (valid) {
-                    float* oa = out + (long long)(2 * l) * NA * a.es;
-                    float* ob = oa + (long long)NA * a.es;
+                    float* oa = out + (long long)(2 * l) * NA * ES;
+                    float* ob = oa + (long long)NA * ES;
+                    const float sc = a.scale;
 #pragma unroll
                     for (int j = 0; j < LA::M; ++j)
 #pragma unroll
                         for (int k = 0; k < LA::N2; ++k) {
                             const int i1 = (p + LA::N2 * j) + LA::N1 * k;
-                            oa[i1 * a.es] = v[j * LA::N2 + k].x * a.scale;
-                            ob[i1 * a.es] = v[j * LA::N2 + k].y * a.scale;
+                            oa[i1 * ES] = v[j * LA::N2 + k].x * sc;
+                            ob[i1 * ES] = v[j * LA::N2 + k].y * sc;
                         }
                 }
             }
@@ -361,11 +359,15 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
     }
 }
 
-// Synthesis / rfft slab pass (forward): real volumes -> spectra (the box rows).
-template <int NA, int NB, int MINB>
+// Synthesis / rfft slab pass (forward): real volumes (element stride ES) ->
+// spectra (the box rows).
+template <int NA, int NB, int ES, int MINB>
 __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArgs a) {
     using LA = SlabLine<NA>;
     using LB = SlabLine<NB>;
+    constexpr int P1 = slab_pitch_c(NA / 2 + 1);
+    constexpr int SL = P1 * NB;
+    constexpr long long PLANE = (long long)NA * NB;
     constexpr int H1 = NA / 2 + 1;
     constexpr int QA = (H1 + LA::N2 - 1) / LA::N2;   // output bins a lane unpacks
     extern __shared__ float2 sm[];
@@ -376,38 +378,35 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
     load_slab_twiddles<NB>(twB, a.twb);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int P1 = a.P1;
-    const int SL = P1 * NB;
-    const long long plane = (long long)NA * NB;
+    const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
         const int z = u / a.n3, s3 = u - z * a.n3;
         // 1. R2C along axis 1 of columns 2l, 2l+1 (as the real and imaginary parts of one line)
         {
-            const int p = lane % LA::N2, s = pair_subline<NA>(lane / LA::N2);
+            const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
             constexpr int npairs = NB / 2;
-            const float* in = a.vol + a.vz.off(z) + (long long)s3 * plane * a.es;
+            const float* in = a.vol + a.vz.off(z) + (long long)s3 * PLANE * ES;
             for (int base = 0; base < npairs; base += LA::LPR) {
                 if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
                 const int l = base + warp * LA::LPW + s;
                 const bool valid = l < npairs;
-                const float* ia = in + (long long)(2 * (valid ? l : 0)) * NA * a.es;
-                const float* ib = ia + (long long)NA * a.es;
+                const float* ia = in + (long long)(2 * (valid ? l : 0)) * NA * ES;
+                const float* ib = ia + (long long)NA * ES;
                 float2 v[LA::N1];
 #pragma unroll
                 for (int r = 0; r < LA::N1; ++r) {
                     const int i = p + LA::N2 * r;
-                    v[r] = valid ? make_float2(ia[i * a.es], ib[i * a.es]) : make_float2(0.f, 0.f);
+                    v[r] = valid ? make_float2(ia[i * ES], ib[i * ES]) : make_float2(0.f, 0.f);
                 }
                 float2* ca = S + P1 * (2 * (valid ? l : 0));
                 float2* cb = ca + P1;
-                const PairSlot slot{ca, cb, (NA + 1) / 2};
-                warp_line_fft<NA, false>(v, p, valid, twA, slot);
+                warp_line_fft<NA, false, 1>(v, p, valid, twA, ca);
                 // Z in natural order through the pair's slots, then the two half spectra
                 if (valid) {
 #pragma unroll
                     for (int j = 0; j < LA::M; ++j)
 #pragma unroll
-                        for (int k = 0; k < LA::N2; ++k) *slot((p + LA::N2 * j) + LA::N1 * k) = v[j * LA::N2 + k];
+                        for (int k = 0; k < LA::N2; ++k) ca[(p + LA::N2 * j) + LA::N1 * k] = v[j * LA::N2 + k];
                 }
                 __syncwarp();
                 float2 ha[QA], hb[QA];
@@ -415,9 +414,9 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
                 for (int q = 0; q < QA; ++q) {
                     const int k = p + LA::N2 * q;
                     ha[q] = hb[q] = make_float2(0.f, 0.f);
-                    if (valid && k < a.nk1) {
-                        const float2 zk = *slot(k);
-                        const float2 zn = *slot(k == 0 ? 0 : NA - k);
+                    if (valid && k < nk1) {
+                        const float2 zk = ca[k];
+                        const float2 zn = ca[k == 0 ? 0 : NA - k];
                         ha[q] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
                         hb[q] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
                     }
@@ -427,7 +426,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
 #pragma unroll
                     for (int q = 0; q < QA; ++q) {
                         const int k = p + LA::N2 * q;
-                        if (k < a.nk1) {
+                        if (k < nk1) {
                             ca[k] = ha[q];
                             cb[k] = hb[q];
                         }
@@ -438,16 +437,16 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
         __syncthreads();
         // 2. forward FFT along axis 2 of the rows k1 < nk1
         {
-            const int p = lane % LB::N2, s = lane / LB::N2;
-            for (int base = 0; base < a.nk1; base += LB::LPR) {
-                if (base + warp * LB::LPW >= a.nk1) continue;   // warp-uniform
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
                 const int k1 = base + warp * LB::LPW + s;
-                const bool valid = k1 < a.nk1;
+                const bool valid = k1 < nk1;
                 float2* row = S + (valid ? k1 : 0);
                 float2 v[LB::N1];
 #pragma unroll
                 for (int r = 0; r < LB::N1; ++r) v[r] = valid ? row[P1 * (p + LB::N2 * r)] : make_float2(0.f, 0.f);
-                warp_line_fft<NB, false>(v, p, valid, twB, RowSlot{row, P1});
+                warp_line_fft<NB, false, P1>(v, p, valid, twB, row);
                 if (valid) {
 #pragma unroll
                     for (int j = 0; j < LB::M; ++j)
@@ -459,9 +458,9 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
         __syncthreads();
         // 3. the box of the slab out to the spectrum
         float2* dst = a.spec + z * a.spec_zstride + (long long)s3 * SL;
-        for (int j = warp; j < a.nk2; j += kSlabWarps) {
-            const int k2 = j <= a.b2 ? j : j + (NB - a.nk2);
-            for (int k1 = lane; k1 < a.nk1; k1 += 32) dst[k1 + P1 * k2] = S[k1 + P1 * k2];
+        for (int j = warp; j < nk2; j += kSlabWarps) {
+            const int k2 = j <= b2 ? j : j + (NB - nk2);
+            for (int k1 = lane; k1 < nk1; k1 += 32) dst[k1 + P1 * k2] = S[k1 + P1 * k2];
         }
         __syncthreads();   // the slab buffer is reused by the next unit
     }
@@ -475,10 +474,10 @@ constexpr int slab_minb() {
 }
 
 // One CTA a unit up to the resident capacity; CTAs stride over the rest.
-template <bool INV, int NA, int NB>
-void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
+template <bool INV, int NA, int NB, int ES>
+void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     constexpr int MINB = (slab_minb<NA>() == 2 && slab_minb<NB>() == 2) ? 2 : 1;
-    auto kern = INV ? ns_slab_inv_kernel<NA, NB, MINB> : ns_slab_fwd_kernel<NA, NB, MINB>;
+    auto kern = INV ? ns_slab_inv_kernel<NA, NB, ES, MINB> : ns_slab_fwd_kernel<NA, NB, ES, MINB>;
     static size_t configured = 0;
     static int resident = 0;
     if (configured < smem) {
@@ -494,6 +493,15 @@ void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, co
     kern<<<grid, kSlabThreads, smem, st>>>(a);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "slab kernel launch");
+}
+
+template <bool INV, int NA, int NB>
+void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
+    if (a.P1 != slab_pitch_c(NA / 2 + 1)) throw ArgError("slab pitch mismatch");
+    if (a.es == 1)
+        launch_slab_es<INV, NA, NB, 1>(a, sms, smem, st, tag);
+    else
+        launch_slab_es<INV, NA, NB, 2>(a, sms, smem, st, tag);
 }
 
 template <bool INV, int NA>
@@ -521,11 +529,7 @@ void launch_slab(int na, int nb, const SlabArgs& a, int sms, size_t smem, cudaSt
 
 bool slab_len(int n) { return n == 64 || n == 96 || n == 128 || n == 160; }
 
-int slab_pitch(int h1) {
-    int p = h1;
-    while (p % 4 != 2) ++p;
-    return p;
-}
+int slab_pitch(int h1) { return slab_pitch_c(h1); }
 
 size_t slab_smem(int n1, int n2) { return sizeof(float2) * ((size_t)n1 + n2 + (size_t)slab_pitch(n1 / 2 + 1) * n2); }
 
