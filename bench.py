@@ -175,6 +175,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip plain/secondary/cpu legs")
     ap.add_argument("--group", type=int, default=0, help="subbands in flight per launch (0: the plan's default)")
+    ap.add_argument("--mode", default="graph", choices=["graph", "calls"],
+                    help="graph: the batch as one CUDA graph over up to 4 workspaces (sfl_batch_*); "
+                         "calls: a loop of plain calls on one workspace")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))
@@ -194,9 +197,12 @@ def main():
     B = args.batch
     N = int(np.prod(DIMS))
     t = sfl.NSSurfacelet(**NS_KW)
-    ws = sfl.make_workspace(t, "float32", DIMS)
-    if args.group > 0:
-        ws.set_group(args.group)
+    nws = min(4, B) if args.mode == "graph" else 1
+    wss = [sfl.make_workspace(t, "float32", DIMS) for _ in range(nws)]
+    for w in wss:
+        if args.group > 0:
+            w.set_group(args.group)
+    ws = wss[0]
     S = ws.nsubbands
     gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
     xs = [sfl.volume_like(DIMS).copy_(torch.randn(DIMS, device="cuda", generator=gen)) for _ in range(B)]
@@ -204,11 +210,23 @@ def main():
     gs = [sfl.volume_like(DIMS + (S,)) for _ in range(B)]
     ys = [sfl.volume_like(DIMS) for _ in range(B)]
 
-    def step():
+    def step_calls():
         for b in range(B):
             sfl.analyze_(cs[b], ws, xs[b])
             sfl.synthesize_(ys[b], ws, cs[b])
             sfl.adjoint_synthesize_(gs[b], ws, ys[b])
+
+    if args.mode == "graph":
+        # volume b on workspace b mod 4: analyze, synthesize, adjoint in order on its branch
+        ents = [(wss[b % nws], op, i, o) for b in range(B)
+                for op, i, o in (("analyze", xs[b], cs[b]), ("synthesize", cs[b], ys[b]),
+                                 ("adjoint_synthesize", ys[b], gs[b]))]
+        batch = sfl.Batch([e[0] for e in ents], [e[2] for e in ents], [e[3] for e in ents], [e[1] for e in ents])
+
+        def step():
+            batch.run()
+    else:
+        step = step_calls
 
     def barrier():
         if world > 1:
@@ -251,7 +269,7 @@ def main():
     lib.sfl_profile_enable(1)
     prof_steps = 2
     for _ in range(prof_steps):
-        step()
+        step_calls()
     torch.cuda.synchronize()
     lib.sfl_profile_enable(0)
     import ctypes as C
@@ -295,6 +313,10 @@ def main():
                                "analyze+synthesize+adjoint(synthesize) per volume",
                    "batch_per_gpu": B, "global_batch": B * world, "volume": list(DIMS),
                    "parallelism": f"replicas x{world} (no collective)",
+                   "execution": ("one CUDA graph a step (sfl_batch_*): volume b on workspace b mod "
+                                 f"{nws}, workspaces on concurrent branches" if args.mode == "graph"
+                                 else "a loop of plain calls on one workspace"),
+                   "kernel_times": "CUDA events around every launch, from a replay as plain calls",
                    "l2": "inputs larger than L2 (411 MB of coefficients a volume)"},
         "gpu_launches": launches_per_step * args.steps,
         "rel_err": {"perfect_reconstruction_rel_l2": rel_pr, "adjoint_vs_analyze_rel_l2": rel_adj},
@@ -317,14 +339,12 @@ def main():
     hy = [torch.empty(DIMS[::-1], dtype=torch.float32).pin_memory() for _ in range(B)]
     for b in range(B):
         hx[b].copy_(xs[b].permute(2, 1, 0))
-    dx = [sfl.volume_like(DIMS) for _ in range(B)]
 
     def e2e_step():
         for b in range(B):
-            dx[b].permute(2, 1, 0).copy_(hx[b], non_blocking=True)
-            sfl.analyze_(cs[b], ws, dx[b])
-            sfl.synthesize_(ys[b], ws, cs[b])
-            sfl.adjoint_synthesize_(gs[b], ws, ys[b])
+            xs[b].permute(2, 1, 0).copy_(hx[b], non_blocking=True)
+        step()
+        for b in range(B):
             hy[b].copy_(ys[b].permute(2, 1, 0), non_blocking=True)
 
     e2e_step()

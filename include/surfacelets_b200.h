@@ -270,9 +270,10 @@ int sfl_ns_analyze_bf16(sfl_plan* plan, const void* x, void* c, float* scales, v
 int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, void* x, void* stream);
 
 /* ── Batches ─────────────────────────────────────────────────────────────
- * Many transforms as one CUDA graph: batch_create runs each (plan, input,
- * output) once eagerly, then captures the sequence (distinct plans on up to
- * four concurrent branches; transforms of one plan keep their order) and
+ * Many transforms as one CUDA graph: batch_create runs each entry (plan,
+ * operator, input, output) once eagerly, then captures the sequence
+ * (distinct plans on up to four concurrent branches; the entries of one plan
+ * keep their order, so an entry may consume an earlier one's output) and
  * instantiates it; batch_run replays it on a stream with the same pointers,
  * whose contents may change between runs.  The plans must stay alive and
  * must not be used elsewhere while a run is in flight.  No counterpart in the
@@ -282,8 +283,8 @@ typedef struct sfl_batch sfl_batch;
 #define SFL_OP_SYNTHESIZE 1
 #define SFL_OP_ADJOINT_ANALYZE 2
 #define SFL_OP_ADJOINT_SYNTHESIZE 3
-int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* inputs, void* const* outputs,
-                     int32_t op, sfl_batch** out);
+int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, const void* const* inputs,
+                     void* const* outputs, sfl_batch** out);
 int sfl_batch_run(sfl_batch* batch, void* stream);
 int sfl_batch_destroy(sfl_batch* batch);
 

@@ -96,7 +96,7 @@ SIGNATURES = {
     "sfl_ns_inverse_spectrum": (C.c_int, [P, P, P, P]),
     "sfl_ns_analyze_bf16": (C.c_int, [P, P, P, P, P]),
     "sfl_ns_synthesize_bf16": (C.c_int, [P, P, P, P, P]),
-    "sfl_batch_create": (C.c_int, [C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.c_int32,
+    "sfl_batch_create": (C.c_int, [C.c_int32, C.POINTER(P), C.POINTER(C.c_int32), C.POINTER(P), C.POINTER(P),
                                    C.POINTER(P)]),
     "sfl_batch_run": (C.c_int, [P, P]),
     "sfl_batch_destroy": (C.c_int, [P]),

@@ -1,10 +1,12 @@
 """Batches of transforms replayed as one CUDA graph (sfl_batch_*).
 
 The reference runs a batch of volumes as a loop of plain analyze!/synthesize!
-calls.  Here `Batch(workspaces, inputs, outputs, op)` runs each transform once,
+calls.  Here `Batch(workspaces, inputs, outputs, ops)` runs each entry once,
 captures the whole sequence into a CUDA graph (distinct workspaces on up to
-four concurrent branches) and `run()` replays it: one launch for the batch.
-The tensors stay bound to the graph; refill the inputs in place between runs.
+four concurrent branches; the entries of one workspace keep their order, so
+one entry may consume another's output) and `run()` replays it: one launch
+for the batch.  The tensors stay bound to the graph; refill the inputs in
+place between runs.
 """
 
 import ctypes as C
@@ -17,23 +19,26 @@ OPS = {"analyze": 0, "synthesize": 1, "adjoint_analyze": 2, "adjoint_synthesize"
 
 
 class Batch:
-    def __init__(self, workspaces, inputs, outputs, op="analyze"):
-        if op not in OPS:
-            raise ArgumentError(f"unknown operator {op!r}; expected one of {sorted(OPS)}")
+    """ops: one operator name for every entry, or one per entry."""
+
+    def __init__(self, workspaces, inputs, outputs, ops="analyze"):
         n = len(workspaces)
-        if n < 1 or len(inputs) != n or len(outputs) != n:
-            raise ArgumentError("a batch needs as many inputs and outputs as workspaces (at least one)")
-        for ws, a, b in zip(workspaces, inputs, outputs):
+        ops = [ops] * n if isinstance(ops, str) else list(ops)
+        if n < 1 or len(inputs) != n or len(outputs) != n or len(ops) != n:
+            raise ArgumentError("a batch needs as many operators, inputs and outputs as workspaces (at least one)")
+        for ws, op, a, b in zip(workspaces, ops, inputs, outputs):
+            if op not in OPS:
+                raise ArgumentError(f"unknown operator {op!r}; expected one of {sorted(OPS)}")
             if not isinstance(ws, Workspace):
                 raise ArgumentError("batch members must be workspaces (make_workspace)")
             vol, coef = (a, b) if op in ("analyze", "adjoint_synthesize") else (b, a)
             _check_device_array(vol, "volume", ws.dims, ws.dtype)
             _check_device_array(coef, "coefficients", _coef_shape(ws), ws.dtype)
-        self.workspaces, self.inputs, self.outputs, self.op = list(workspaces), list(inputs), list(outputs), op
+        self.workspaces, self.inputs, self.outputs, self.ops = list(workspaces), list(inputs), list(outputs), ops
         arr = C.c_void_p * n
         h = C.c_void_p()
-        check(lib.sfl_batch_create(n, arr(*[w._h for w in workspaces]), arr(*[_ptr(a) for a in inputs]),
-                                   arr(*[_ptr(b) for b in outputs]), OPS[op], C.byref(h)))
+        check(lib.sfl_batch_create(n, arr(*[w._h for w in workspaces]), (C.c_int32 * n)(*[OPS[o] for o in ops]),
+                                   arr(*[_ptr(a) for a in inputs]), arr(*[_ptr(b) for b in outputs]), C.byref(h)))
         self._h = h
 
     def run(self, stream=None):

@@ -794,17 +794,16 @@ int sfl_ns_inverse_spectrum(sfl_plan* plan, void* A, void* x, void* stream) {
 
 // ── batches: one CUDA graph over many transforms ─────────────────────────────
 
-int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* inputs, void* const* outputs,
-                     int32_t op, sfl_batch** out) {
+int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, const void* const* inputs,
+                     void* const* outputs, sfl_batch** out) {
     return guarded([&] {
         need(plans, "plans");
+        need(ops, "ops");
         need(inputs, "inputs");
         need(outputs, "outputs");
         need(out, "out");
         *out = nullptr;
         if (n < 1) throw sfl::ArgError("a batch needs at least one transform, got " + std::to_string(n));
-        if (op < SFL_OP_ANALYZE || op > SFL_OP_ADJOINT_SYNTHESIZE)
-            throw sfl::ArgError("unknown operator " + std::to_string(op));
         const int dev = (need(plans[0], "plans[0]"), plans[0]->impl.device);
         // distinct plans run on up to kBranches concurrent branches; one plan always on the same branch
         constexpr int kBranches = 4;
@@ -812,6 +811,8 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* input
         std::vector<int> branch(n);
         for (int i = 0; i < n; ++i) {
             need(plans[i], "plans[i]");
+            if (ops[i] < SFL_OP_ANALYZE || ops[i] > SFL_OP_ADJOINT_SYNTHESIZE)
+                throw sfl::ArgError("unknown operator " + std::to_string(ops[i]));
             need(inputs[i], "inputs[i]");
             need(outputs[i], "outputs[i]");
             if (plans[i]->impl.device != dev) throw sfl::ArgError("the plans of a batch must share one device");
@@ -844,14 +845,14 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const void* const* input
                 sfl::cuda_check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
                 for (auto& e : join) sfl::cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
                 // one eager pass: validates the arguments and configures every kernel outside the capture
-                for (int i = 0; i < n; ++i) run_op(plans[i], op, inputs[i], outputs[i], s[0]);
+                for (int i = 0; i < n; ++i) run_op(plans[i], ops[i], inputs[i], outputs[i], s[0]);
                 sfl::cuda_check(cudaStreamSynchronize(s[0]), "batch warm-up");
                 sfl_profile_enable(0);
                 sfl::cuda_check(cudaStreamBeginCapture(s[0], cudaStreamCaptureModeThreadLocal), "begin capture");
                 try {
                     sfl::cuda_check(cudaEventRecord(fork, s[0]), "fork");
                     for (int k = 1; k < kBranches; ++k) sfl::cuda_check(cudaStreamWaitEvent(s[k], fork, 0), "fork");
-                    for (int i = 0; i < n; ++i) run_op(plans[i], op, inputs[i], outputs[i], s[branch[i]]);
+                    for (int i = 0; i < n; ++i) run_op(plans[i], ops[i], inputs[i], outputs[i], s[branch[i]]);
                     for (int k = 1; k < kBranches; ++k) {
                         sfl::cuda_check(cudaEventRecord(join[k], s[k]), "join");
                         sfl::cuda_check(cudaStreamWaitEvent(s[0], join[k], 0), "join");

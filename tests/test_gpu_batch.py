@@ -66,5 +66,28 @@ def test_batch_argument_errors(sfl):
         sfl.Batch(wss, xs[:1], cs, "analyze")
     with pytest.raises(sfl.ArgumentError):
         sfl.Batch(wss, xs, cs, "transpose")
+    with pytest.raises(sfl.ArgumentError):
+        sfl.Batch(wss, xs, cs, ["analyze"])
     with pytest.raises(sfl.DimensionMismatch):
         sfl.Batch(wss, xs[::-1], cs, "analyze")
+
+
+def test_batch_chains_operators_of_one_workspace(sfl):
+    # analyze -> synthesize -> adjoint of synthesize per workspace, in one graph
+    wss = _members(sfl)[:5]
+    rng = np.random.default_rng(12)
+    ents, refs = [], []
+    for ws in wss:
+        x = sfl.to_device(rng.standard_normal(ws.dims).astype(np.float32))
+        c, y, g = _coef(sfl, ws), sfl.volume_like(ws.dims), _coef(sfl, ws)
+        ents += [(ws, "analyze", x, c), (ws, "synthesize", c, y), (ws, "adjoint_synthesize", y, g)]
+        refs.append((ws, x, c, y, g))
+    b = sfl.Batch([e[0] for e in ents], [e[2] for e in ents], [e[3] for e in ents], [e[1] for e in ents])
+    b.run()
+    torch.cuda.synchronize()
+    for ws, x, c, y, g in refs:
+        c0 = sfl.analyze(ws, x)
+        y0 = sfl.synthesize(ws, c0)
+        assert torch.equal(c, c0) and torch.equal(y, y0)
+        assert torch.equal(g, sfl.adjoint_synthesize(ws, y0))
+    b.close()
