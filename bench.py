@@ -175,6 +175,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip plain/secondary/cpu legs")
     ap.add_argument("--group", type=int, default=0, help="subbands in flight per launch (0: the plan's default)")
+    ap.add_argument("--workspaces", type=int, default=4, help="graph mode: workspaces (concurrent branches, <= 8)")
     ap.add_argument("--mode", default="graph", choices=["graph", "calls"],
                     help="graph: the batch as one CUDA graph over up to 4 workspaces (sfl_batch_*); "
                          "calls: a loop of plain calls on one workspace")
@@ -197,7 +198,7 @@ def main():
     B = args.batch
     N = int(np.prod(DIMS))
     t = sfl.NSSurfacelet(**NS_KW)
-    nws = min(4, B) if args.mode == "graph" else 1
+    nws = min(args.workspaces, B) if args.mode == "graph" else 1
     wss = [sfl.make_workspace(t, "float32", DIMS) for _ in range(nws)]
     for w in wss:
         if args.group > 0:

@@ -806,7 +806,7 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, cons
         if (n < 1) throw sfl::ArgError("a batch needs at least one transform, got " + std::to_string(n));
         const int dev = (need(plans[0], "plans[0]"), plans[0]->impl.device);
         // distinct plans run on up to kBranches concurrent branches; one plan always on the same branch
-        constexpr int kBranches = 4;
+        constexpr int kBranches = 8;
         std::vector<const sfl_plan*> distinct;
         std::vector<int> branch(n);
         for (int i = 0; i < n; ++i) {
