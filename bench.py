@@ -325,7 +325,7 @@ def main():
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "peak_kind": peak_kind,
                      "launches_per_step": dom_launches, "ms_per_step": dom_ms,
-                     "share_of_step": dom_ms / ms},
+                     "share_of_kernel_time": dom_ms / sum(v[0] for v in per_tag.values())},
         "op_roofline": {"algorithmic_bytes_per_voxel": 600, "achieved_gbs": op_bytes / (ms / 1e3) / 1e9 / world,
                         "frac": op_bytes / (ms / 1e3) / 1e9 / world / hbm, "peak_kind": peak_kind},
         "kernel_ms_per_step": {k: v[0] for k, v in per_tag.items()},
