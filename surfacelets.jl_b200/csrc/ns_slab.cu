@@ -120,6 +120,63 @@ struct L3LoadMask {
     }
 };
 
+// Analysis line pass over IPC subbands of one mask group per CTA: a line's X
+// times the group factor is loaded once, then per subband scaled by its two
+// wedge planes, transformed along axis 3 and stored.
+template <int N, int IPC>
+__global__ void __launch_bounds__(256) ns_slab_mask_group_kernel(const float2* __restrict__ X, int P1, int s3,
+                                                                 BoxMap bx, NSMaskTables tb,
+                                                                 const NSItem* __restrict__ items, int item0, int nz,
+                                                                 int synth, float2* Y, long long ystride,
+                                                                 const float2* __restrict__ tw, int nlines) {
+    using Ge = RegGeom<N>;
+    constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
+    extern __shared__ float2 xch[];
+    const int tid = threadIdx.x;
+    const int lp = tid % LP, p = tid / LP;
+    const int l = blockIdx.x * LP + lp;
+    const bool valid = l < nlines;
+    int k1 = 0, k2 = 0;
+    if (valid) bx.k12(l, k1, k2);
+    float2* xl = xch + lp * Ge::XLINE;
+    const long long si = (long long)tb.h1 * tb.n2;
+    const int lnat = k1 + tb.h1 * k2;
+    const int z0 = blockIdx.y * IPC;
+    // the group factor of the line (group table, bandpass table or the lowpass factors)
+    const NSMaskLine m0 = ns_mask_line(tb, items[item0 + z0], lnat, synth != 0);
+    const float2* xp = X + k1 + P1 * k2;
+    float2 xg[N1];
+#pragma unroll
+    for (int r = 0; r < N1; ++r) {
+        const int i = p + N2 * r;
+        const float g = m0.low ? m0.lowc * m0.lowv[i] : m0.m[i * si];
+        xg[r] = valid ? c_scale(xp[(long long)i * s3], g) : make_float2(0.f, 0.f);
+    }
+#pragma unroll 1
+    for (int zz = 0; zz < IPC; ++zz) {
+        const int z = z0 + zz;
+        if (z >= nz) break;   // uniform across the CTA
+        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
+        const bool wedges = !(mk.low || mk.plain);
+        float2 v[N1];
+#pragma unroll
+        for (int r = 0; r < N1; ++r) {
+            const int i = p + N2 * r;
+            v[r] = wedges ? c_scale(xg[r], mk.wa[i * mk.was] * mk.wb[i * mk.wbs]) : xg[r];
+        }
+        float2 u[E];
+        reg_line_fft_v<N, true>(v, p, xl, tw, u);
+        if (valid) {
+            float2* y = Y + z * ystride + k1 + P1 * k2;
+#pragma unroll
+            for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+                for (int k = 0; k < N2; ++k) y[((p + N2 * j) + N1 * k) * s3] = u[j * N2 + k];
+        }
+        __syncthreads();   // the exchange rows are reused by the next subband
+    }
+}
+
 // Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
 // summed in registers into the accumulator (plain float32 sums, item order).
 template <int N>
@@ -145,18 +202,33 @@ __global__ void __launch_bounds__(256, 2) ns_slab_accum_kernel(const float2* __r
         for (int k = 0; k < N2; ++k)
             s[j * N2 + k] = valid ? a[((p + N2 * j) + N1 * k) * s3] : make_float2(0.f, 0.f);
     const long long si_nat = (long long)tb.h1 * tb.n2;
-    for (int z = 0; z < G; ++z) {
-        L3LoadC ld{Y + z * ystride, 0, P1, s3, bx};
-        L3LoadC::Ctx lc{ld.src + k1 + P1 * k2};
-        float2 u[E];
-        reg_line_fft<N, false>(ld, lc, valid, p, xl, tw, u);
-        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], k1 + tb.h1 * k2, synth != 0);
+    const int lnat = k1 + tb.h1 * k2;
+    // the group factor of the line (group table, bandpass table or the lowpass factors), once for all items
+    float gf[E];
+    {
+        const NSMaskLine m0 = ns_mask_line(tb, items[item0], lnat, synth != 0);
 #pragma unroll
         for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
             for (int k = 0; k < N2; ++k) {
                 const int k3 = (p + N2 * j) + N1 * k;
-                s[j * N2 + k] = c_add(s[j * N2 + k], c_scale(u[j * N2 + k], ns_mask_at(mk, k3, si_nat)));
+                gf[j * N2 + k] = m0.low ? m0.lowc * m0.lowv[k3] : m0.m[k3 * si_nat];
+            }
+    }
+    for (int z = 0; z < G; ++z) {
+        L3LoadC ld{Y + z * ystride, 0, P1, s3, bx};
+        L3LoadC::Ctx lc{ld.src + k1 + P1 * k2};
+        float2 u[E];
+        reg_line_fft<N, false>(ld, lc, valid, p, xl, tw, u);
+        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
+        const bool wedges = !(mk.low || mk.plain);
+#pragma unroll
+        for (int j = 0; j < Ge::M; ++j)
+#pragma unroll
+            for (int k = 0; k < N2; ++k) {
+                const int k3 = (p + N2 * j) + N1 * k;
+                const float m = wedges ? gf[j * N2 + k] * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]) : gf[j * N2 + k];
+                s[j * N2 + k] = c_add(s[j * N2 + k], c_scale(u[j * N2 + k], m));
             }
         __syncthreads();   // the exchange rows are reused by the next item
     }
@@ -584,6 +656,40 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
     cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
 }
 
+template <int N, int IPC>
+void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
+                           int nlines, cudaStream_t st) {
+    using Ge = RegGeom<N>;
+    static bool configured = false;
+    if (!configured) {
+        cuda_check(cudaFuncSetAttribute(ns_slab_mask_group_kernel<N, IPC>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ge::SMEM),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    dim3 grid((nlines + Ge::LP - 1) / Ge::LP, (nz + IPC - 1) / IPC);
+    int tok = prof_begin("ns_slab_mask_axis3", st);
+    ns_slab_mask_group_kernel<N, IPC><<<grid, Ge::THREADS, Ge::SMEM, st>>>(
+        X, P.P1, P.P1 * P.dims[1], bx, P.tb, P.items.as<NSItem>(), i0, nz, synth, Y, P.SP,
+        P.ffts.at(P.dims[2])->sh.tw, nlines);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "ns_slab_mask_group_kernel launch");
+}
+
+// Subbands a CTA of the analysis line pass takes: the line's X and group
+// factor are loaded once for all of them.
+int mask_ipc(int nz) { return nz >= 4 ? 4 : (nz >= 2 ? 2 : 1); }
+
+template <int N>
+void launch_mask_group(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
+                       int nlines, cudaStream_t st) {
+    switch (mask_ipc(nz)) {
+        case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, st); return;
+        case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, st); return;
+        default: launch_mask_group_ipc<N, 1>(P, X, Y, nz, bx, i0, synth, nlines, st); return;
+    }
+}
+
 // Algorithmic bytes of one box of a spectrum (complex float32 bins).
 double box_bytes(const NSPlan& P, const NSBox& b) { return 8.0 * b.nk1 * b.nk2 * P.dims[2]; }
 
@@ -633,8 +739,19 @@ void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es,
     // X and the group table once, the nz spectra out; then those back in and nz volumes out
     prof_bytes("ns_slab_mask_axis3", 1.5 * box_bytes(P, b) + nz * box_bytes(P, b));
     prof_bytes("ns_slab_c2r", nz * (box_bytes(P, b) + 4.0 * P.N));
-    line3<true>(P, L3LoadMask{X, P.P1, s3, bx, P.tb, P.items.as<NSItem>(), i0, synth_masks ? 1 : 0},
-                L3StoreC{Y, P.SP, P.P1, s3, bx}, b.nk1 * b.nk2, nz, st, "ns_slab_mask_axis3");
+    {
+        const int nl = b.nk1 * b.nk2, sy = synth_masks ? 1 : 0;
+        switch (P.dims[2]) {
+            case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, st); break;
+            default: throw ArgError("no register line pass for axis 3 of this size");
+        }
+    }
     SlabArgs a = slab_args(P, b, nz);
     a.spec = Y;
     a.spec_zstride = P.SP;

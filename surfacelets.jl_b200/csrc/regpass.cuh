@@ -226,15 +226,13 @@ struct RStoreFullPair {
 // One line of N points per N2 threads: load, in-register DFT_N1, twiddle,
 // exchange, in-register DFT_N2 (M per thread).  Leaves the outputs in
 // u[j * N2 + k] = X[(p + N2 j) + N1 k].
-template <int N, bool INV, class Load>
-__device__ __forceinline__ void reg_line_fft(const Load& ld, const typename Load::Ctx& lc, bool valid, int p,
-                                             float2* xl, const float2* __restrict__ tw,
-                                             float2 (&u)[RegGeom<N>::M * RegGeom<N>::N2]) {
+// The same from values already in registers: v[r] = x[p + N2 r].
+template <int N, bool INV>
+__device__ __forceinline__ void reg_line_fft_v(float2 (&v)[RegGeom<N>::N1], int p, float2* xl,
+                                               const float2* __restrict__ tw,
+                                               float2 (&u)[RegGeom<N>::M * RegGeom<N>::N2]) {
     using G = RegGeom<N>;
     constexpr int N1 = G::N1, N2 = G::N2;
-    float2 v[N1];
-#pragma unroll
-    for (int r = 0; r < N1; ++r) v[r] = valid ? ld.get(lc, p + N2 * r) : make_float2(0.f, 0.f);
     RegDft<N1, INV>::run(v);
 #pragma unroll
     for (int m = 1; m < N1; ++m) {
@@ -255,6 +253,18 @@ __device__ __forceinline__ void reg_line_fft(const Load& ld, const typename Load
 #pragma unroll
         for (int k = 0; k < N2; ++k) u[j * N2 + k] = w[k];
     }
+}
+
+template <int N, bool INV, class Load>
+__device__ __forceinline__ void reg_line_fft(const Load& ld, const typename Load::Ctx& lc, bool valid, int p,
+                                             float2* xl, const float2* __restrict__ tw,
+                                             float2 (&u)[RegGeom<N>::M * RegGeom<N>::N2]) {
+    using G = RegGeom<N>;
+    constexpr int N1 = G::N1, N2 = G::N2;
+    float2 v[N1];
+#pragma unroll
+    for (int r = 0; r < N1; ++r) v[r] = valid ? ld.get(lc, p + N2 * r) : make_float2(0.f, 0.f);
+    reg_line_fft_v<N, INV>(v, p, xl, tw, u);
 }
 
 template <int N, bool INV, class Load, class Store>
