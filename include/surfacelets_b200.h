@@ -54,6 +54,7 @@ extern "C" {
 
 #define SFL_KIND_NS 0
 #define SFL_KIND_DECIMATED 1
+#define SFL_KIND_NDFB 2        /* standalone directional bank (make_ndfb / make_hourglass) */
 
 /* NSSurfacelet(; scales, direction_levels, bernstein_order, halfband_order,
  *              transition, tight) — src/types/transforms.jl:86-113.
@@ -66,6 +67,18 @@ typedef struct {
     double transition;
     int32_t tight;
 } sfl_ns_params;
+
+/* make_ndfb(dims; levels, bernstein_order, halfband_order, tight, transition)
+ * — src/directional/ndfb.jl:91-104; levels = 0 is make_hourglass
+ * (src/directional/hourglass.jl:149-170).  3 * 2^levels full-size subbands,
+ * index ((i-1) na + (p-1)) nb + q (src/directional/ndfb.jl:184-190). */
+typedef struct {
+    int32_t levels;
+    int32_t bernstein_order;
+    int32_t halfband_order;
+    double transition;
+    int32_t tight;
+} sfl_ndfb_params;
 
 /* Surfacelet(; scales, direction_levels, pyramid_ratio, checkerboard_order,
  *            diamond_length, kaiser_beta, diamond_power) —
@@ -128,6 +141,15 @@ int sfl_surf_redundancy(const sfl_surf_params* p, const int32_t dims[3], double*
  * Designs the masks in float64, stores them as float32 on the current device
  * and allocates the scratch.  dtype is SFL_REAL32 or SFL_COMPLEX64. */
 int sfl_ns_plan_create(const sfl_ns_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out);
+
+/* The standalone directional bank on the NSSurfacelet kernels: parameter
+ * check (host only; "levels must be ≥ 0", "transition must be ≥ 0" as in
+ * src/directional/ndfb.jl:98-99) and plan.  The plan takes sfl_analyze
+ * (ndfb_decompose!, src/directional/ndfb.jl:276), sfl_synthesize
+ * (ndfb_reconstruct!, :384), the adjoints and the streaming entry points
+ * (ndfb_decompose(f, ...), :317); coefficients are (n1, n2, n3, 3 * 2^levels). */
+int sfl_ndfb_check_params(const sfl_ndfb_params* p);
+int sfl_ndfb_plan_create(const sfl_ndfb_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out);
 
 /* make_workspace(t::Surfacelet, T, dims): src/transforms/surfacelet.jl:126-149. */
 int sfl_surf_plan_create(const sfl_surf_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out);

@@ -48,6 +48,17 @@ class SurfParams(C.Structure):
     ]
 
 
+class NDFBParams(C.Structure):
+    """sfl_ndfb_params"""
+    _fields_ = [
+        ("levels", C.c_int32),
+        ("bernstein_order", C.c_int32),
+        ("halfband_order", C.c_int32),
+        ("transition", C.c_double),
+        ("tight", C.c_int32),
+    ]
+
+
 Dims = C.c_int32 * 3
 P = C.c_void_p
 
@@ -65,6 +76,8 @@ SIGNATURES = {
                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "sfl_surf_redundancy": (C.c_int, [C.POINTER(SurfParams), Dims, C.POINTER(C.c_double)]),
     "sfl_ns_plan_create": (C.c_int, [C.POINTER(NSParams), Dims, C.c_int32, C.POINTER(P)]),
+    "sfl_ndfb_check_params": (C.c_int, [C.POINTER(NDFBParams)]),
+    "sfl_ndfb_plan_create": (C.c_int, [C.POINTER(NDFBParams), Dims, C.c_int32, C.POINTER(P)]),
     "sfl_surf_plan_create": (C.c_int, [C.POINTER(SurfParams), Dims, C.c_int32, C.POINTER(P)]),
     "sfl_plan_destroy": (C.c_int, [P]),
     "sfl_plan_info": (C.c_int, [P, C.POINTER(C.c_int32), Dims, C.POINTER(C.c_int32), C.POINTER(C.c_int32),

@@ -283,6 +283,50 @@ int sfl_ns_plan_create(const sfl_ns_params* p, const int32_t dims[3], int32_t dt
     });
 }
 
+static sfl_ns_params ndfb_as_ns(const sfl_ndfb_params& p) {
+    if (p.levels < 0) throw sfl::ArgError("levels must be ≥ 0");
+    if (!(p.transition >= 0)) throw sfl::ArgError("transition must be ≥ 0");
+    sfl_ns_params q{};
+    q.scales = 1;
+    q.direction_levels[0] = p.levels;
+    q.bernstein_order = p.bernstein_order;
+    q.halfband_order = p.halfband_order;
+    q.transition = p.transition;
+    q.tight = p.tight;
+    sfl::ns_check_params(q);
+    return q;
+}
+
+int sfl_ndfb_check_params(const sfl_ndfb_params* p) {
+    return guarded([&] {
+        need(p, "params");
+        ndfb_as_ns(*p);
+        return SFL_OK;
+    });
+}
+
+int sfl_ndfb_plan_create(const sfl_ndfb_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out) {
+    return guarded([&] {
+        need(p, "params");
+        need(out, "out");
+        *out = nullptr;
+        if (dtype != SFL_REAL32 && dtype != SFL_COMPLEX64) throw sfl::ArgError("dtype must be SFL_REAL32 or SFL_COMPLEX64");
+        int d[3];
+        dims_of(dims, d);
+        const sfl_ns_params q = ndfb_as_ns(*p);
+        for (int i = 0; i < 3; ++i)
+            if (d[i] < 1) throw sfl::DimError("volume size must be positive");
+        std::unique_ptr<sfl_plan> plan(new sfl_plan);
+        plan->impl.kind = SFL_KIND_NS;
+        plan->impl.dtype = dtype;
+        sfl::cuda_check(cudaGetDevice(&plan->impl.device), "cudaGetDevice");
+        plan->impl.ns.reset(new sfl::NSPlan);
+        sfl::ns_plan_init(*plan->impl.ns, q, d, dtype, true);
+        *out = plan.release();
+        return SFL_OK;
+    });
+}
+
 int sfl_surf_plan_create(const sfl_surf_params* p, const int32_t dims[3], int32_t dtype, sfl_plan** out) {
     return guarded([&] {
         need(p, "params");
@@ -325,7 +369,7 @@ int sfl_plan_info(const sfl_plan* plan, int32_t* kind, int32_t dims[3], int32_t*
     return guarded([&] {
         need(plan, "plan");
         const sfl::Plan& P = plan->impl;
-        if (kind) *kind = P.kind;
+        if (kind) *kind = P.kind == SFL_KIND_NS && P.ns->ndfb ? SFL_KIND_NDFB : P.kind;
         if (dtype) *dtype = P.dtype;
         if (P.kind == SFL_KIND_NS) {
             const sfl::NSPlan& N = *P.ns;

@@ -351,9 +351,9 @@ static void hourglass_tables(const int dims[3], int order, int poly, std::vector
 }
 
 // src/transforms/ns_surfacelet.jl:98-123, 178-185
-NSDesign ns_design(const sfl_ns_params& p, const int dims[3]) {
+NSDesign ns_design(const sfl_ns_params& p, const int dims[3], bool pyramid) {
     ns_check_params(p);
-    ns_check_size(p, dims);
+    if (pyramid) ns_check_size(p, dims);
     NSDesign D;
     for (int d = 0; d < 3; ++d) D.dims[d] = dims[d];
     D.h1 = dims[0] / 2 + 1;
@@ -380,6 +380,24 @@ NSDesign ns_design(const sfl_ns_params& p, const int dims[3]) {
     for (int lv = 0; lv < p.scales; ++lv)
         for (int d = 0; d < 3; ++d) D.pl[lv][d] = prof[d][lv];
     return D;
+}
+
+// The hourglass mask of the standalone bank: sqrt(W_i) when tight, W_i
+// otherwise (src/directional/hourglass.jl:264-303, 400-412).
+std::vector<double> ns_hourglass_mask(const NSDesign& D, int i) {
+    const int h1 = D.h1, n2 = D.dims[1], n3 = D.dims[2];
+    std::vector<double> G((size_t)h1 * n2 * n3);
+    for (int k3 = 0; k3 < n3; ++k3)
+        for (int k2 = 0; k2 < n2; ++k2)
+            for (int k1 = 0; k1 < h1; ++k1) {
+                size_t q = k1 + (size_t)h1 * (k2 + (size_t)n2 * k3);
+                double f1 = D.m1[q], f2 = D.m2[k2 + (size_t)n2 * k3];
+                double w1 = i == 1 ? f1 : 1 - f1;
+                double w2 = i == 1 ? 1.0 : (i == 2 ? f2 : 1 - f2);
+                double w = w1 * w2;
+                G[q] = D.p.tight ? std::sqrt(std::max(w, 0.0)) : w;
+            }
+    return G;
 }
 
 // src/transforms/ns_surfacelet.jl:265-272 (_hg_factor, _bandpass), 278-303

@@ -77,7 +77,9 @@ void ns_check_params(const sfl_ns_params& p);
 void ns_check_size(const sfl_ns_params& p, const int dims[3]);
 int ns_nbands(const sfl_ns_params& p, int j);      // scale j 1-based
 int ns_nsubbands(const sfl_ns_params& p);
-NSDesign ns_design(const sfl_ns_params& p, const int dims[3]);
+// pyramid = false: the standalone directional bank (no pyramid, no size rule).
+NSDesign ns_design(const sfl_ns_params& p, const int dims[3], bool pyramid = true);
+std::vector<double> ns_hourglass_mask(const NSDesign& D, int i);
 
 // ── Decimated Surfacelet ──────────────────────────────────────────────────────
 

@@ -263,9 +263,11 @@ void ns_use_planes(NSPlan& P) {
         };
         std::vector<float> Gp, Blp;
         for (int j = 1; j <= J; ++j)
-            for (int i = 1; i <= 3; ++i) permute(ns_group_mask(D, J - j, i, true), Gp);
+            for (int i = 1; i <= 3; ++i)
+                permute(P.ndfb ? ns_hourglass_mask(D, i) : ns_group_mask(D, J - j, i, true), Gp);
         if (!P.p.tight)
-            for (int lv = 0; lv < J; ++lv) permute(ns_group_mask(D, lv, 1, false), Blp);
+            for (int lv = 0; lv < J; ++lv)
+                permute(P.ndfb ? std::vector<double>((size_t)P.H, 1.0) : ns_group_mask(D, lv, 1, false), Blp);
         upload(P.Gp, Gp);
         upload(P.Blp, Blp);
         P.tbp = P.tb;
@@ -279,17 +281,21 @@ void ns_use_planes(NSPlan& P) {
     }
 }
 
-void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype) {
+// With ndfb, the standalone directional bank of one level count
+// (src/directional/ndfb.jl:91-104; HourglassFB at level 0): the same cascade
+// with the hourglass masks alone as group factors, no pyramid and no lowpass.
+void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype, bool ndfb) {
     for (int d = 0; d < 3; ++d)
         if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
-    P.design = ns_design(p, dims);
+    P.ndfb = ndfb;
+    P.design = ns_design(p, dims, !ndfb);
     const NSDesign& D = P.design;
     P.p = p;
     for (int d = 0; d < 3; ++d) P.dims[d] = dims[d];
     P.h1 = dims[0] / 2 + 1;
     P.N = (long long)dims[0] * dims[1] * dims[2];
     P.H = (long long)P.h1 * dims[1] * dims[2];
-    P.S = ns_nsubbands(p);
+    P.S = ndfb ? 3 * (1 << p.direction_levels[0]) : ns_nsubbands(p);
     P.nch = dtype == SFL_COMPLEX64 ? 2 : 1;
     const int J = p.scales;
 
@@ -301,23 +307,32 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
         P.boxes.clear();
         for (int j = 1; j <= J; ++j)
             for (int i = 1; i <= 3; ++i) {
-                std::vector<double> g = ns_group_mask(D, J - j, i, true);
+                std::vector<double> g = ndfb ? ns_hourglass_mask(D, i) : ns_group_mask(D, J - j, i, true);
                 for (double v : g) G.push_back((float)v);
                 P.boxes.push_back(ns_table_box(g, P.h1, dims[1], dims[2]));
             }
         upload(P.G, G);
         std::vector<float> Bl;
-        if (!p.tight)
-            for (int lv = 0; lv < J; ++lv) {
-                std::vector<double> b = ns_group_mask(D, lv, 1, false);
-                for (double v : b) Bl.push_back((float)v);
-                // the synthesis bandpass B_j covers the group factors of its level
-                const NSBox bb = ns_table_box(b, P.h1, dims[1], dims[2]);
-                for (int i = 0; i < 3; ++i) P.boxes[3 * (J - 1 - lv) + i] = bb;
+        if (!p.tight) {
+            if (ndfb) {
+                // untight synthesis filters of the standalone bank are all 1
+                Bl.assign((size_t)P.H, 1.0f);
+            } else {
+                for (int lv = 0; lv < J; ++lv) {
+                    std::vector<double> b = ns_group_mask(D, lv, 1, false);
+                    for (double v : b) Bl.push_back((float)v);
+                    // the synthesis bandpass B_j covers the group factors of its level
+                    const NSBox bb = ns_table_box(b, P.h1, dims[1], dims[2]);
+                    for (int i = 0; i < 3; ++i) P.boxes[3 * (J - 1 - lv) + i] = bb;
+                }
             }
+        }
         upload(P.Bl, Bl);
     }
-    {
+    if (ndfb) {
+        P.boxes.push_back(ns_make_box(P.h1, dims[1], dims[1]));   // no lowpass; keeps the table indexing uniform
+        P.boxes_full = ns_make_box(P.h1, dims[1], dims[1]);
+    } else {
         // lowpass box from its per-axis factors
         int m1 = -1, m2 = -1;
         const auto& a1 = D.pa[J][0];
@@ -332,7 +347,10 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     std::vector<float> vec;
     for (int d = 0; d < 3; ++d) {
         tb.low_off[d] = (int)vec.size();
-        for (double x : D.pa[J][d]) vec.push_back((float)x);
+        if (ndfb)
+            vec.resize(vec.size() + (d == 0 ? P.h1 : dims[d]), 1.0f);
+        else
+            for (double x : D.pa[J][d]) vec.push_back((float)x);
     }
     upload(P.vec, vec);
     std::vector<float> planes;
@@ -361,7 +379,7 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     // items in streaming order: directional subbands ascending, then the lowpass.
     // Subband index: src/transforms/ns_surfacelet.jl:222-242, 430
     std::vector<NSItem> items;
-    int offset = 1;
+    int offset = ndfb ? 0 : 1;   // the bank's subband index: ((i-1) na + (p-1)) nb + q, src/directional/ndfb.jl:184-190
     for (int j = 1; j <= J; ++j) {
         int L = p.direction_levels[j - 1];
         int na = 1 << ((L + 1) / 2), nb = 1 << (L / 2);
@@ -388,12 +406,14 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
                 }
         offset += 3 * na * nb;
     }
-    NSItem low{};
-    low.s = 1;
-    low.kind = 1;
-    low.lv = J;
-    low.i = 1;
-    items.push_back(low);
+    if (!ndfb) {
+        NSItem low{};
+        low.s = 1;
+        low.kind = 1;
+        low.lv = J;
+        low.i = 1;
+        items.push_back(low);
+    }
     P.items_host = items;
     upload(P.items, items);
 

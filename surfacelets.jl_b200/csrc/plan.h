@@ -105,6 +105,7 @@ struct NSPlan {
     long long H = 0;      // rfft grid points
     int S = 0;            // subbands
     int nch = 1;          // 1 real, 2 complex
+    bool ndfb = false;    // the standalone directional bank (no pyramid, no lowpass)
     int group = 8;
     std::vector<NSItem> items_host;   // streaming / item order: directional ascending, then lowpass
     DevMem items;
@@ -151,7 +152,7 @@ struct Plan {
 FFTLen* get_fft(std::map<int, std::unique_ptr<FFTLen>>& cache, int n);
 
 // NS drivers (ns.cu)
-void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype);
+void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype, bool ndfb = false);
 void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
 void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
 void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);

@@ -94,6 +94,85 @@ class NSSurfacelet:
                 f"transition = {_fmt_real(self.transition)}, tight = {'true' if self.tight else 'false'})")
 
 
+class NDFB(NSSurfacelet):
+    """The standalone nonsubsampled directional filter bank (make_ndfb,
+    src/directional/ndfb.jl:91-104): 3 * 2^levels full-size subbands, the
+    hourglass bank refined into wedges, run on the NSSurfacelet kernels with
+    no pyramid and no lowpass.  levels = 0 is the hourglass bank."""
+
+    def __init__(self, levels=2, bernstein_order=12, halfband_order=1, tight=True, transition=1.0):
+        if isinstance(levels, (bool, np.bool_)) or not isinstance(levels, (int, np.integer)):
+            raise ArgumentError(f"levels must be an integer, got {levels!r}")
+        self.levels = int(levels)
+        self.scales = 1
+        self.direction_levels = [self.levels]
+        self.bernstein_order = int(bernstein_order)
+        self.halfband_order = int(halfband_order)
+        self.transition = float(transition) + 0.0
+        self.tight = bool(tight)
+        check(lib.sfl_ndfb_check_params(C.byref(self._ndfb_params())))
+
+    def _ndfb_params(self):
+        p = _lib.NDFBParams()
+        p.levels = self.levels
+        p.bernstein_order = self.bernstein_order
+        p.halfband_order = self.halfband_order
+        p.transition = self.transition
+        p.tight = 1 if self.tight else 0
+        return p
+
+    def _key(self):
+        return ("NDFB", self.levels, self.bernstein_order, self.halfband_order, self.transition, self.tight)
+
+    def __eq__(self, other):
+        return isinstance(other, NDFB) and self._key() == other._key()
+
+    def __hash__(self):
+        return hash(self._key())
+
+    def wedge_counts(self):
+        """(na, nb): wedges on the two transverse planes of a hourglass (src/directional/ndfb.jl:146)."""
+        return 1 << ((self.levels + 1) // 2), 1 << (self.levels // 2)
+
+    def __repr__(self):
+        return (f"NDFB(levels = {self.levels}, bernstein_order = {self.bernstein_order}, "
+                f"halfband_order = {self.halfband_order}, tight = {'true' if self.tight else 'false'}, "
+                f"transition = {_fmt_real(self.transition)})")
+
+
+class HourglassFB(NDFB):
+    """The three-subband hourglass bank (make_hourglass, src/directional/hourglass.jl:149-170)."""
+
+    def __init__(self, bernstein_order=12, halfband_order=1, tight=True):
+        super().__init__(0, bernstein_order, halfband_order, tight, 1.0)
+
+    def __repr__(self):
+        return (f"HourglassFB(bernstein_order = {self.bernstein_order}, halfband_order = {self.halfband_order}, "
+                f"tight = {'true' if self.tight else 'false'})")
+
+
+def ndfb_subband_index(t, hourglass, p, q):
+    """src/directional/ndfb.jl:184-190"""
+    na, nb = t.wedge_counts()
+    if not 1 <= hourglass <= 3:
+        raise ArgumentError("hourglass index must be 1, 2 or 3")
+    if not 1 <= p <= na:
+        raise ArgumentError(f"wedge index p out of range 1:{na}")
+    if not 1 <= q <= nb:
+        raise ArgumentError(f"wedge index q out of range 1:{nb}")
+    return ((hourglass - 1) * na + (p - 1)) * nb + q
+
+
+def ndfb_subband_triple(t, idx):
+    """(hourglass, p, q) of subband idx.  src/directional/ndfb.jl:199-203"""
+    na, nb = t.wedge_counts()
+    if not 1 <= idx <= 3 * na * nb:
+        raise ArgumentError("subband index out of range")
+    r, q = divmod(idx - 1, nb)
+    i, p = divmod(r, na)
+    return i + 1, p + 1, q + 1
+
+
 def _level_matrix(L):
     """src/types/transforms.jl:263-284"""
     if isinstance(L, (bool, np.bool_)):
@@ -189,6 +268,8 @@ def _cdims(dims):
 def nsubbands(t, dims):
     """src/transforms/ns_surfacelet.jl:527, src/transforms/surfacelet.jl:310"""
     dims = _dims3(dims)
+    if isinstance(t, NDFB):
+        return 3 << t.levels
     if isinstance(t, NSSurfacelet):
         n = C.c_int32()
         check(lib.sfl_ns_nsubbands(C.byref(t._params()), C.byref(n)))
@@ -204,6 +285,8 @@ def subband_layout(t, dims):
     (dicts with `scale`, `hourglass`, `wedge`)."""
     dims = _dims3(dims)
     n = nsubbands(t, dims)
+    if isinstance(t, NDFB):
+        return [dict(zip(("hourglass", "wedge_a", "wedge_b"), ndfb_subband_triple(t, i))) for i in range(1, n + 1)]
     if isinstance(t, NSSurfacelet):
         sc = (C.c_int32 * n)()
         di = (C.c_int32 * n)()
@@ -217,6 +300,8 @@ def subband_layout(t, dims):
 def subband_sizes(t, dims):
     """Shape of every subband, in layout order."""
     dims = _dims3(dims)
+    if isinstance(t, NDFB):
+        return [dims] * nsubbands(t, dims)
     if isinstance(t, NSSurfacelet):
         check(lib.sfl_ns_check_size(C.byref(t._params()), _cdims(dims)))
         return [dims] * nsubbands(t, dims)
@@ -316,7 +401,9 @@ class Workspace:
         self.dims = _dims3(dims)
         self.dtype = dtype_code
         h = C.c_void_p()
-        if isinstance(t, NSSurfacelet):
+        if isinstance(t, NDFB):
+            check(lib.sfl_ndfb_plan_create(C.byref(t._ndfb_params()), _cdims(self.dims), dtype_code, C.byref(h)))
+        elif isinstance(t, NSSurfacelet):
             check(lib.sfl_ns_plan_create(C.byref(t._params()), _cdims(self.dims), dtype_code, C.byref(h)))
         else:
             check(lib.sfl_surf_plan_create(C.byref(t._params()), _cdims(self.dims), dtype_code, C.byref(h)))
@@ -365,7 +452,8 @@ class Workspace:
         return _dtype_name(self.dtype)
 
     def __repr__(self):
-        name = "NSSurfaceletWorkspace" if isinstance(self.transform, NSSurfacelet) else "SurfaceletWorkspace"
+        name = ("NDFBWorkspace" if isinstance(self.transform, NDFB) else
+                "NSSurfaceletWorkspace" if isinstance(self.transform, NSSurfacelet) else "SurfaceletWorkspace")
         return f"{name}{{{self.eltype}}}({'×'.join(map(str, self.dims))}, {self.transform})"
 
 
@@ -707,3 +795,48 @@ def analyze_synthesize_stream(f, y, x, analysis_workspace, synthesis_workspace, 
         check(lib.sfl_stream_synthesize_push(wsy._h, _ptr(out), st))
     check(lib.sfl_stream_synthesize_end(wsy._h, _ptr(y), st))
     return y
+
+
+# ── the standalone directional banks (src/directional/ndfb.jl, hourglass.jl) ─
+
+
+def ndfb_decompose(ws, x, stream=None):
+    """All 3 * 2^levels subbands of x, as one (n1, n2, n3, S) array (subband
+    idx at [..., idx-1]).  src/directional/ndfb.jl:263-285"""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NDFB):
+        raise ArgumentError("ndfb_decompose needs an NDFB workspace")
+    return analyze(ws, x, stream=stream)
+
+
+def ndfb_reconstruct(ws, c, stream=None):
+    """src/directional/ndfb.jl:384-410"""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NDFB):
+        raise ArgumentError("ndfb_reconstruct needs an NDFB workspace")
+    return synthesize(ws, c, stream=stream)
+
+
+def hourglass_decompose(ws, x, stream=None):
+    """(s1, s2, s3).  src/directional/hourglass.jl:330-358"""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NDFB) or ws.transform.levels != 0:
+        raise ArgumentError("hourglass_decompose needs a HourglassFB workspace")
+    c = analyze(ws, x, stream=stream)
+    return tuple(c[..., i] for i in range(3))
+
+
+def hourglass_reconstruct(ws, subbands, stream=None):
+    """src/directional/hourglass.jl:435-459"""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NDFB) or ws.transform.levels != 0:
+        raise ArgumentError("hourglass_reconstruct needs a HourglassFB workspace")
+    if len(subbands) != 3:
+        raise ArgumentError(f"a hourglass bank has 3 subbands, got {len(subbands)}")
+    for i, b in enumerate(subbands, start=1):
+        if tuple(b.shape) != ws.dims:
+            raise DimensionMismatch(f"subband {i} has size {tuple(b.shape)}, expected {ws.dims}")
+    if torch is not None and isinstance(subbands[0], torch.Tensor):
+        c = volume_like(ws.dims + (3,), "complex64" if ws.dtype else "float32", subbands[0].device)
+        for i, b in enumerate(subbands):
+            c[..., i].copy_(b)
+    else:
+        c = np.stack([np.asarray(b) for b in subbands], axis=-1)
+        c = np.asfortranarray(c)
+    return synthesize(ws, c, stream=stream)
