@@ -408,6 +408,34 @@ def main():
                              "perfect_reconstruction_rel_l2": rel_dec,
                              "algorithmic_bytes_per_voxel": 4 * 2 * (1 + wd.ncoeffs / N)}
 
+        # downstream consumer: the fused soft-threshold denoiser against the three calls
+        tau = 0.05
+        yn = sfl.volume_like(DIMS)
+
+        def den_step():
+            for b in range(B):
+                yn.copy_(sfl.denoise(ws, xs[b], tau))
+
+        tt = torch.full((S,), tau, device="cuda")
+        tt[0] = 0
+
+        def three_step():
+            for b in range(B):
+                sfl.analyze_(cs[b], ws, xs[b])
+                cs[b].copy_(torch.sign(cs[b]) * torch.clamp(cs[b].abs() - tt, min=0))
+                sfl.synthesize_(ys[b], ws, cs[b])
+
+        for _ in range(2):
+            den_step()
+            three_step()
+        ms_den = timed(den_step, max(3, args.steps // 2))
+        ms_three = timed(three_step, max(3, args.steps // 2))
+        line["denoiser"] = {"workload": "soft threshold 0.05 of every directional subband, same NSSurfacelet "
+                                        "128^3, one workspace, plain calls",
+                            "fused_value": B * N / (ms_den / 1e3) / 1e6,
+                            "three_calls_value": B * N / (ms_three / 1e3) / 1e6, "unit": "Mvoxels/s",
+                            "equal_bit_for_bit": bool(torch.equal(yn, ys[B - 1]))}
+
         # CPU baseline: the oracle port on the host cores, bounded sample
         from oracle.cpu_baseline import NSBaseline
         cores = os.cpu_count()

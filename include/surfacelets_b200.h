@@ -260,6 +260,14 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
 int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name,
                           int32_t index, double* out, int64_t* count);
 
+/* ── Soft-threshold denoiser (NSSurfacelet and NDFB plans, Float32) ─────
+ * No counterpart in the reference.  y = synthesize(soft(analyze(x), tau)),
+ * soft(c) = sign(c) max(|c| - tau[s-1], 0) on subband s; tau is S float32
+ * thresholds in device memory, by subband index.  On the slab pipeline the
+ * coefficients never reach device memory (analysis, threshold and synthesis
+ * of a subband meet in one slab pass); equal bit for bit to the three calls. */
+int sfl_ns_denoise(sfl_plan* plan, const void* x, void* y, const float* tau, void* stream);
+
 /* ── Item ranges (NSSurfacelet; sharding subbands across devices) ────────
  * No counterpart in the reference.  The subbands in stream order (stream_order
  * gives the subband index at each of the S positions) split into ranges:

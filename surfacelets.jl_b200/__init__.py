@@ -15,7 +15,7 @@ from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateEr
 from .transforms import (  # noqa: F401
     NDFB, HourglassFB, NSSurfacelet, Surfacelet, Workspace, adjoint_analyze, hourglass_decompose,
     hourglass_reconstruct, ndfb_decompose, ndfb_reconstruct, ndfb_subband_index, ndfb_subband_triple, adjoint_analyze_, adjoint_synthesize,
-    adjoint_synthesize_, analyze, analyze_, analyze_bf16, analyze_synthesize_stream, synthesize_bf16, checkerboard_orders, make_workspace, nsubbands,
+    adjoint_synthesize_, analyze, analyze_, analyze_bf16, denoise, analyze_synthesize_stream, synthesize_bf16, checkerboard_orders, make_workspace, nsubbands,
     similar_coefficients, subband, subband_layout, subband_sizes, supports_streaming, surfacelet_redundancy,
     synthesize, synthesize_, to_device, to_host, volume_like,
 )

@@ -718,6 +718,22 @@ int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, v
     });
 }
 
+int sfl_ns_denoise(sfl_plan* plan, const void* x, void* y, const float* tau, void* stream) {
+    return guarded([&] {
+        need(x, "x");
+        need(y, "y");
+        need(tau, "tau");
+        sfl::NSPlan& N = ns_of(plan, "the denoiser");
+        if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(y, plan->impl.dtype, "y");
+        on_device(plan, [&] {
+            sfl::ns_denoise(N, static_cast<const float*>(x), static_cast<float*>(y), tau, as_stream(stream));
+        });
+        return SFL_OK;
+    });
+}
+
 // ── item ranges (sharding subbands across devices) ──────────────────────────
 
 static sfl::NSPlan& range_plan(sfl_plan* plan) {

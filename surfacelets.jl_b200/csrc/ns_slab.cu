@@ -254,6 +254,9 @@ struct SlabArgs {
     int units;               // items x n3
     const float2* twa;       // w_n1^k, k < n1 (float64-designed)
     const float2* twb;       // w_n2^k, k < n2
+    const float* tau;        // shrink pass: threshold of subband s at tau[s - 1]
+    const NSItem* items;     // shrink pass: the launch's items, from item0
+    int item0;
 };
 
 template <int N>
@@ -538,6 +541,167 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
     }
 }
 
+// The denoiser's slab pass (real data): per slab of Y_s, the analysis half
+// (inverse FFT along axis 2, C2R along axis 1, 1/N) gives the subband's slab
+// in registers; it is soft-thresholded, c' = sign(c) max(|c| - tau_s, 0), and
+// the synthesis half (R2C along axis 1, FFT along axis 2 of the box rows)
+// writes the box back into the same slab of Y_s.  The subband itself never
+// leaves the chip.  Same arithmetic, in the same order, as analyze ->
+// threshold -> synthesize through the two slab passes.
+template <int NA, int NB, int MINB>
+__global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_shrink_kernel(SlabArgs a) {
+    using LA = SlabLine<NA>;
+    using LB = SlabLine<NB>;
+    constexpr int P1 = slab_pitch_c(NA / 2 + 1);
+    constexpr int SL = P1 * NB;
+    constexpr int H1 = NA / 2 + 1;
+    constexpr int QA = (H1 + LA::N2 - 1) / LA::N2;
+    extern __shared__ float2 sm[];
+    float2* twA = sm;
+    float2* twB = sm + NA;
+    float2* S = sm + NA + NB;
+    load_slab_twiddles<NA>(twA, a.twa);
+    load_slab_twiddles<NB>(twB, a.twb);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
+    const int k2hi = NB - (nk2 - b2 - 1);
+    for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
+        const int z = u / a.n3, s3 = u - z * a.n3;
+        float2* slab = a.spec + z * a.spec_zstride + (long long)s3 * SL;
+        const float tau = a.tau[a.items[a.item0 + z].s - 1];
+        for (int j = warp; j < nk2; j += kSlabWarps) {
+            const int k2 = j <= b2 ? j : j + (NB - nk2);
+            for (int k1 = lane; k1 < nk1; k1 += 32) S[k1 + P1 * k2] = slab[k1 + P1 * k2];
+        }
+        __syncthreads();
+        {   // inverse FFT along axis 2 of the box rows
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) {
+                    const int k2 = p + LB::N2 * r;
+                    const bool in = valid && (k2 <= b2 || k2 >= k2hi);
+                    v[r] = in ? row[P1 * k2] : make_float2(0.f, 0.f);
+                }
+                warp_line_fft<NB, true, P1>(v, p, valid, twB, row);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
+        __syncthreads();
+        {   // per column pair: C2R, threshold, R2C
+            const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
+            constexpr int npairs = NB / 2;
+            for (int base = 0; base < npairs; base += LA::LPR) {
+                if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
+                const int l = base + warp * LA::LPW + s;
+                const bool valid = l < npairs;
+                float2* ca = S + P1 * (2 * (valid ? l : 0));
+                float2* cb = ca + P1;
+                float2 v[LA::N1];
+#pragma unroll
+                for (int r = 0; r < LA::N1; ++r) {
+                    const int i = p + LA::N2 * r;
+                    const int k = 2 * i <= NA ? i : NA - i;
+                    float2 A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
+                    if (valid && k < nk1) {
+                        A = ca[k];
+                        B = cb[k];
+                    }
+                    if (k == 0 || 2 * k == NA) {
+                        A.y = 0.f;
+                        B.y = 0.f;
+                    }
+                    v[r] = 2 * i <= NA ? make_float2(A.x - B.y, A.y + B.x) : make_float2(A.x + B.y, B.x - A.y);
+                }
+                warp_line_fft<NA, true, 1>(v, p, valid, twA, ca);
+                // the two subband columns, thresholded, in natural order through the pair's slots
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LA::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LA::N2; ++k) {
+                            const float2 c = v[j * LA::N2 + k];
+                            const float xa = c.x * a.scale, xb = c.y * a.scale;
+                            ca[(p + LA::N2 * j) + LA::N1 * k] =
+                                make_float2(copysignf(fmaxf(fabsf(xa) - tau, 0.f), xa),
+                                            copysignf(fmaxf(fabsf(xb) - tau, 0.f), xb));
+                        }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < LA::N1; ++r) v[r] = valid ? ca[p + LA::N2 * r] : make_float2(0.f, 0.f);
+                warp_line_fft<NA, false, 1>(v, p, valid, twA, ca);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LA::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LA::N2; ++k) ca[(p + LA::N2 * j) + LA::N1 * k] = v[j * LA::N2 + k];
+                }
+                __syncwarp();
+                float2 ha[QA], hb[QA];
+#pragma unroll
+                for (int q = 0; q < QA; ++q) {
+                    const int k = p + LA::N2 * q;
+                    ha[q] = hb[q] = make_float2(0.f, 0.f);
+                    if (valid && k < nk1) {
+                        const float2 zk = ca[k];
+                        const float2 zn = ca[k == 0 ? 0 : NA - k];
+                        ha[q] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+                        hb[q] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+                    }
+                }
+                __syncwarp();
+                if (valid) {
+#pragma unroll
+                    for (int q = 0; q < QA; ++q) {
+                        const int k = p + LA::N2 * q;
+                        if (k < nk1) {
+                            ca[k] = ha[q];
+                            cb[k] = hb[q];
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        {   // forward FFT along axis 2 of the box rows
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) v[r] = valid ? row[P1 * (p + LB::N2 * r)] : make_float2(0.f, 0.f);
+                warp_line_fft<NB, false, P1>(v, p, valid, twB, row);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
+        __syncthreads();
+        for (int j = warp; j < nk2; j += kSlabWarps) {
+            const int k2 = j <= b2 ? j : j + (NB - nk2);
+            for (int k1 = lane; k1 < nk1; k1 += 32) slab[k1 + P1 * k2] = S[k1 + P1 * k2];
+        }
+        __syncthreads();   // the slab buffer is reused by the next unit
+    }
+}
+
 // ── launch tables ────────────────────────────────────────────────────────────
 
 template <int N>
@@ -546,10 +710,12 @@ constexpr int slab_minb() {
 }
 
 // One CTA a unit up to the resident capacity; CTAs stride over the rest.
-template <bool INV, int NA, int NB, int ES>
+// KIND: 0 the forward slab pass, 1 the inverse, 2 the denoiser's shrink pass.
+template <int KIND, int NA, int NB, int ES>
 void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     constexpr int MINB = (slab_minb<NA>() == 2 && slab_minb<NB>() == 2) ? 2 : 1;
-    auto kern = INV ? ns_slab_inv_kernel<NA, NB, ES, MINB> : ns_slab_fwd_kernel<NA, NB, ES, MINB>;
+    auto kern = KIND == 1 ? ns_slab_inv_kernel<NA, NB, ES, MINB>
+                          : (KIND == 0 ? ns_slab_fwd_kernel<NA, NB, ES, MINB> : ns_slab_shrink_kernel<NA, NB, MINB>);
     static size_t configured = 0;
     static int resident = 0;
     if (configured < smem) {
@@ -567,34 +733,34 @@ void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, co
     cuda_check(cudaGetLastError(), "slab kernel launch");
 }
 
-template <bool INV, int NA, int NB>
+template <int KIND, int NA, int NB>
 void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     if (a.P1 != slab_pitch_c(NA / 2 + 1)) throw ArgError("slab pitch mismatch");
     if (a.es == 1)
-        launch_slab_es<INV, NA, NB, 1>(a, sms, smem, st, tag);
+        launch_slab_es<KIND, NA, NB, 1>(a, sms, smem, st, tag);
     else
-        launch_slab_es<INV, NA, NB, 2>(a, sms, smem, st, tag);
+        launch_slab_es<KIND, NA, NB, 2>(a, sms, smem, st, tag);
 }
 
-template <bool INV, int NA>
+template <int KIND, int NA>
 bool launch_slab_n(int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     switch (nb) {
-        case 64: launch_slab_nn<INV, NA, 64>(a, sms, smem, st, tag); return true;
-        case 96: launch_slab_nn<INV, NA, 96>(a, sms, smem, st, tag); return true;
-        case 128: launch_slab_nn<INV, NA, 128>(a, sms, smem, st, tag); return true;
-        case 160: launch_slab_nn<INV, NA, 160>(a, sms, smem, st, tag); return true;
+        case 64: launch_slab_nn<KIND, NA, 64>(a, sms, smem, st, tag); return true;
+        case 96: launch_slab_nn<KIND, NA, 96>(a, sms, smem, st, tag); return true;
+        case 128: launch_slab_nn<KIND, NA, 128>(a, sms, smem, st, tag); return true;
+        case 160: launch_slab_nn<KIND, NA, 160>(a, sms, smem, st, tag); return true;
     }
     return false;
 }
 
-template <bool INV>
+template <int KIND>
 void launch_slab(int na, int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     bool ok = false;
     switch (na) {
-        case 64: ok = launch_slab_n<INV, 64>(nb, a, sms, smem, st, tag); break;
-        case 96: ok = launch_slab_n<INV, 96>(nb, a, sms, smem, st, tag); break;
-        case 128: ok = launch_slab_n<INV, 128>(nb, a, sms, smem, st, tag); break;
-        case 160: ok = launch_slab_n<INV, 160>(nb, a, sms, smem, st, tag); break;
+        case 64: ok = launch_slab_n<KIND, 64>(nb, a, sms, smem, st, tag); break;
+        case 96: ok = launch_slab_n<KIND, 96>(nb, a, sms, smem, st, tag); break;
+        case 128: ok = launch_slab_n<KIND, 128>(nb, a, sms, smem, st, tag); break;
+        case 160: ok = launch_slab_n<KIND, 160>(nb, a, sms, smem, st, tag); break;
     }
     if (!ok) throw ArgError("no slab kernel for this size");
 }
@@ -702,7 +868,7 @@ void slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
     a.spec = X;
     a.vol = const_cast<float*>(x);
     a.es = es;
-    launch_slab<false>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
+    launch_slab<0>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
                        "ns_slab_r2c");
     const BoxMap bx = box_map(P, full);
     const int s3 = P.P1 * P.dims[1];
@@ -724,62 +890,35 @@ void slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) {
     a.vol = x;
     a.es = es;
     a.scale = 1.0f / (float)P.N;
-    launch_slab<true>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
+    launch_slab<1>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
                       "ns_slab_c2r");
 }
 
-// Analysis of items [i0, i0 + nz) (one mask group) from X into volumes at
-// vol + vz.off(z).
-void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
-                        cudaStream_t st) {
+// The analysis axis-3 pass of items [i0, i0 + nz) (one mask group): X times
+// each mask, inverse FFT along axis 3, into Y (the plan's work spectra).
+void slab_mask_pass(NSPlan& P, const float2* X, int i0, int nz, bool synth_masks, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     const BoxMap bx = box_map(P, b);
-    const int s3 = P.P1 * P.dims[1];
     float2* Y = P.work.as<float2>();
-    // X and the group table once, the nz spectra out; then those back in and nz volumes out
     prof_bytes("ns_slab_mask_axis3", 1.5 * box_bytes(P, b) + nz * box_bytes(P, b));
-    prof_bytes("ns_slab_c2r", nz * (box_bytes(P, b) + 4.0 * P.N));
-    {
-        const int nl = b.nk1 * b.nk2, sy = synth_masks ? 1 : 0;
-        switch (P.dims[2]) {
-            case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, st); break;
-            default: throw ArgError("no register line pass for axis 3 of this size");
-        }
+    const int nl = b.nk1 * b.nk2, sy = synth_masks ? 1 : 0;
+    switch (P.dims[2]) {
+        case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, st); return;
     }
-    SlabArgs a = slab_args(P, b, nz);
-    a.spec = Y;
-    a.spec_zstride = P.SP;
-    a.vol = vol;
-    a.vz = vz;
-    a.es = es;
-    a.scale = 1.0f / (float)P.N;
-    launch_slab<true>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
-                      "ns_slab_c2r");
+    throw ArgError("no register line pass for axis 3 of this size");
 }
 
-// Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
-// vol + vz.off(z) into acc.
-void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
-                      float2* acc, cudaStream_t st) {
+// The synthesis axis-3 pass of items [i0, i0 + nz) from Y into acc.
+void slab_accum_pass(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
-    float2* Y = P.work.as<float2>();
-    // nz volumes in, nz box spectra out; then those in, the group table once and the accumulator in and out
-    prof_bytes("ns_slab_r2c", nz * (4.0 * P.N + box_bytes(P, b)));
+    const float2* Y = P.work.as<float2>();
     prof_bytes("ns_slab_accum_axis3", nz * box_bytes(P, b) + 0.5 * box_bytes(P, b) + 2 * box_bytes(P, b));
-    SlabArgs a = slab_args(P, b, nz);
-    a.spec = Y;
-    a.spec_zstride = P.SP;
-    a.vol = const_cast<float*>(vol);
-    a.vz = vz;
-    a.es = es;
-    launch_slab<false>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
-                       "ns_slab_r2c");
     const BoxMap bx = box_map(P, b);
     const int nl = b.nk1 * b.nk2;
     const int sy = analysis_masks ? 0 : 1;
@@ -793,6 +932,57 @@ void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int 
         case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
     }
     throw ArgError("no register line pass for axis 3 of this size");
+}
+
+// Analysis of items [i0, i0 + nz) (one mask group) from X into volumes at
+// vol + vz.off(z).
+void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
+                        cudaStream_t st) {
+    const NSBox& b = item_box(P, i0);
+    slab_mask_pass(P, X, i0, nz, synth_masks, st);
+    prof_bytes("ns_slab_c2r", nz * (box_bytes(P, b) + 4.0 * P.N));
+    SlabArgs a = slab_args(P, b, nz);
+    a.spec = P.work.as<float2>();
+    a.spec_zstride = P.SP;
+    a.vol = vol;
+    a.vz = vz;
+    a.es = es;
+    a.scale = 1.0f / (float)P.N;
+    launch_slab<1>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_c2r");
+}
+
+// Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
+// vol + vz.off(z) into acc.
+void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                      float2* acc, cudaStream_t st) {
+    const NSBox& b = item_box(P, i0);
+    prof_bytes("ns_slab_r2c", nz * (4.0 * P.N + box_bytes(P, b)));
+    SlabArgs a = slab_args(P, b, nz);
+    a.spec = P.work.as<float2>();
+    a.spec_zstride = P.SP;
+    a.vol = const_cast<float*>(vol);
+    a.vz = vz;
+    a.es = es;
+    launch_slab<0>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_r2c");
+    slab_accum_pass(P, i0, nz, analysis_masks, acc, st);
+}
+
+// The denoiser on items [i0, i0 + nz) (one mask group): the analysis axis-3
+// pass into Y, the shrink slab pass in place, the synthesis accumulation.
+void slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
+                        cudaStream_t st) {
+    const NSBox& b = item_box(P, i0);
+    slab_mask_pass(P, X, i0, nz, false, st);
+    prof_bytes("ns_slab_shrink", nz * 2 * box_bytes(P, b));
+    SlabArgs a = slab_args(P, b, nz);
+    a.spec = P.work.as<float2>();
+    a.spec_zstride = P.SP;
+    a.scale = 1.0f / (float)P.N;
+    a.tau = tau;
+    a.items = P.items.as<NSItem>();
+    a.item0 = i0;
+    launch_slab<2>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_shrink");
+    slab_accum_pass(P, i0, nz, false, acc, st);
 }
 
 // Consecutive items of one mask group, at most P.group of them.
@@ -861,6 +1051,11 @@ void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int 
 void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
                          float2* acc, cudaStream_t st) {
     slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, st);
+}
+
+void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
+                           cudaStream_t st) {
+    slab_denoise_items(P, X, i0, nz, tau, acc, st);
 }
 
 }  // namespace sfl

@@ -177,6 +177,10 @@ void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int 
                            cudaStream_t st);
 void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
                          float2* acc, cudaStream_t st);
+void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
+                           cudaStream_t st);
+// Fused soft-threshold denoiser y = S(soft(A x, tau)) (ns_denoise.cu).
+void ns_denoise(NSPlan& P, const float* x, float* y, const float* tau, cudaStream_t st);
 // Item-range building blocks of the slab and line pipelines (ns.cu): the
 // spectrum of a channel, the launch chunks, the analysis of items into
 // volumes at vol + vz.off(z), their accumulation into a spectrum, and its

@@ -840,3 +840,28 @@ def hourglass_reconstruct(ws, subbands, stream=None):
         c = np.stack([np.asarray(b) for b in subbands], axis=-1)
         c = np.asfortranarray(c)
     return synthesize(ws, c, stream=stream)
+
+
+# ── soft-threshold denoiser ─────────────────────────────────────────────────
+
+
+def denoise(ws, x, tau, stream=None):
+    """y = synthesize(soft(analyze(x), tau)) with soft(c) = sign(c) max(|c| - tau, 0)
+    per subband: tau is one threshold for every directional subband (the
+    lowpass kept), or S thresholds by subband index.  Float32 volumes of an
+    NSSurfacelet or NDFB workspace; on the slab pipeline no coefficient is
+    written to device memory.  Bit for bit the three separate calls."""
+    if not isinstance(ws, Workspace) or not isinstance(ws.transform, NSSurfacelet):
+        raise ArgumentError("the denoiser needs an NSSurfacelet or NDFB workspace")
+    _check_device_array(x, "volume", ws.dims, ws.dtype)
+    if np.ndim(tau) == 0 and not (torch is not None and isinstance(tau, torch.Tensor) and tau.dim() > 0):
+        t = torch.full((ws.nsubbands,), float(tau), dtype=torch.float32, device=x.device)
+        if not isinstance(ws.transform, NDFB):
+            t[0] = 0.0                   # subband 1 is the lowpass
+    else:
+        t = torch.as_tensor(tau, dtype=torch.float32, device=x.device).contiguous()
+        if tuple(t.shape) != (ws.nsubbands,):
+            raise DimensionMismatch(f"{tuple(t.shape)} thresholds, expected ({ws.nsubbands},)")
+    y = volume_like(ws.dims, "float32", x.device)
+    check(lib.sfl_ns_denoise(ws._h, _ptr(x), _ptr(y), _ptr(t), _stream(stream)))
+    return y
