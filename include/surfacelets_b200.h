@@ -313,6 +313,7 @@ typedef struct sfl_batch sfl_batch;
 #define SFL_OP_SYNTHESIZE 1
 #define SFL_OP_ADJOINT_ANALYZE 2
 #define SFL_OP_ADJOINT_SYNTHESIZE 3
+#define SFL_OP_COPY_VOLUME 4   /* copy one volume of the plan's size (host <-> device, pinned host memory) */
 int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, const void* const* inputs,
                      void* const* outputs, sfl_batch** out);
 int sfl_batch_run(sfl_batch* batch, void* stream);

@@ -12,10 +12,12 @@ place between runs.
 import ctypes as C
 
 from . import _lib
-from ._lib import ArgumentError, check, lib
+import numpy as np
+
+from ._lib import ArgumentError, DimensionMismatch, check, lib
 from .transforms import (NSSurfacelet, Workspace, _check_device_array, _coef_shape, _dims3, _ptr, _stream)
 
-OPS = {"analyze": 0, "synthesize": 1, "adjoint_analyze": 2, "adjoint_synthesize": 3}
+OPS = {"analyze": 0, "synthesize": 1, "adjoint_analyze": 2, "adjoint_synthesize": 3, "copy_volume": 4}
 
 
 class Batch:
@@ -31,6 +33,14 @@ class Batch:
                 raise ArgumentError(f"unknown operator {op!r}; expected one of {sorted(OPS)}")
             if not isinstance(ws, Workspace):
                 raise ArgumentError("batch members must be workspaces (make_workspace)")
+            if op == "copy_volume":
+                # a volume between device memory and pinned host memory (or device to device)
+                for t in (a, b):
+                    if t.numel() != int(np.prod(ws.dims)) or t.element_size() != (8 if ws.dtype else 4):
+                        raise DimensionMismatch(f"copy_volume needs {ws.dims} volumes of the workspace's type")
+                    if not t.is_cuda and not t.is_pinned():
+                        raise ArgumentError("copy_volume needs pinned host memory")
+                continue
             vol, coef = (a, b) if op in ("analyze", "adjoint_synthesize") else (b, a)
             _check_device_array(vol, "volume", ws.dims, ws.dtype)
             _check_device_array(coef, "coefficients", _coef_shape(ws), ws.dtype)

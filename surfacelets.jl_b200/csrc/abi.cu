@@ -128,6 +128,17 @@ void run_op(sfl_plan* plan, int op, const void* in, void* out, cudaStream_t st) 
         case SFL_OP_ADJOINT_SYNTHESIZE:
             ns ? sfl::ns_analyze(*P.ns, in, out, st, true) : sfl::dec_adjoint_synthesize(*P.dec, in, out, st);
             return;
+        case SFL_OP_COPY_VOLUME: {
+            int d[3];
+            if (ns) {
+                for (int i = 0; i < 3; ++i) d[i] = P.ns->dims[i];
+            } else {
+                for (int i = 0; i < 3; ++i) d[i] = sfl::dec_design(*P.dec).dims[i];
+            }
+            const size_t bytes = (size_t)d[0] * d[1] * d[2] * (P.dtype == SFL_COMPLEX64 ? 8 : 4);
+            sfl::cuda_check(cudaMemcpyAsync(out, in, bytes, cudaMemcpyDefault, st), "cudaMemcpyAsync(volume)");
+            return;
+        }
     }
     throw sfl::ArgError("unknown operator " + std::to_string(op));
 }
@@ -871,15 +882,17 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, cons
         std::vector<int> branch(n);
         for (int i = 0; i < n; ++i) {
             need(plans[i], "plans[i]");
-            if (ops[i] < SFL_OP_ANALYZE || ops[i] > SFL_OP_ADJOINT_SYNTHESIZE)
+            if (ops[i] < SFL_OP_ANALYZE || ops[i] > SFL_OP_COPY_VOLUME)
                 throw sfl::ArgError("unknown operator " + std::to_string(ops[i]));
             need(inputs[i], "inputs[i]");
             need(outputs[i], "outputs[i]");
             if (plans[i]->impl.device != dev) throw sfl::ArgError("the plans of a batch must share one device");
             if (plans[i]->impl.kind == SFL_KIND_NS && plans[i]->impl.ns->stream_mode != 0)
                 throw sfl::ArgError("a streaming pass is open on a plan of the batch");
-            check_aligned(inputs[i], plans[i]->impl.dtype, "inputs[i]");
-            check_aligned(outputs[i], plans[i]->impl.dtype, "outputs[i]");
+            if (ops[i] != SFL_OP_COPY_VOLUME) {
+                check_aligned(inputs[i], plans[i]->impl.dtype, "inputs[i]");
+                check_aligned(outputs[i], plans[i]->impl.dtype, "outputs[i]");
+            }
             auto it = std::find(distinct.begin(), distinct.end(), plans[i]);
             if (it == distinct.end()) {
                 distinct.push_back(plans[i]);

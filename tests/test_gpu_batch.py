@@ -91,3 +91,27 @@ def test_batch_chains_operators_of_one_workspace(sfl):
         assert torch.equal(c, c0) and torch.equal(y, y0)
         assert torch.equal(g, sfl.adjoint_synthesize(ws, y0))
     b.close()
+
+
+def test_batch_copies_volumes_to_and_from_pinned_host_memory(sfl):
+    wss = _members(sfl)[:3]
+    rng = np.random.default_rng(13)
+    ents, chk = [], []
+    for ws in wss:
+        hx = torch.from_numpy(rng.standard_normal(ws.dims[::-1]).astype(np.float32)).pin_memory()
+        hy = torch.empty(ws.dims[::-1]).pin_memory()
+        x, y, c = sfl.volume_like(ws.dims), sfl.volume_like(ws.dims), _coef(sfl, ws)
+        ents += [(ws, "copy_volume", hx, x), (ws, "analyze", x, c), (ws, "synthesize", c, y),
+                 (ws, "copy_volume", y, hy)]
+        chk.append((ws, hx, hy))
+    b = sfl.Batch([e[0] for e in ents], [e[2] for e in ents], [e[3] for e in ents], [e[1] for e in ents])
+    for _ in range(2):
+        b.run()
+        torch.cuda.synchronize()
+        for ws, hx, hy in chk:
+            xd = hx.cuda().permute(2, 1, 0)              # column-major view of the host volume
+            y0 = sfl.synthesize(ws, sfl.analyze(ws, xd))
+            assert torch.equal(hy.cuda().permute(2, 1, 0), y0)
+    with pytest.raises(sfl.ArgumentError):
+        sfl.Batch([wss[0]], [torch.empty(wss[0].dims[::-1])], [sfl.volume_like(wss[0].dims)], ["copy_volume"])
+    b.close()
