@@ -438,7 +438,7 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
 void ns_alloc_scratch(NSPlan& P) {
     const long long spec = P.slab ? P.SP : P.H;
     P.X.alloc(sizeof(float2) * spec * P.nch);
-    P.work.alloc(sizeof(float2) * spec * P.group);
+    P.work.alloc(sizeof(float2) * spec * P.group * (P.slab ? P.nch : 1));
     if (P.slab) {
         P.acc.alloc(sizeof(float2) * spec * P.nch);
         P.comp.alloc(0);
@@ -647,6 +647,7 @@ ZMap ns_subband_map(const NSPlan& P, int i0, int es) {
 
 void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
     if (P.plane) return ns_plane_analyze(P, x, c, st, synth_masks);
+    if (P.slab) return ns_slab_analyze(P, x, c, st, synth_masks);
     const int es = P.nch;
     float2* X = P.X.as<float2>();
     for (int ch = 0; ch < P.nch; ++ch) {
@@ -661,6 +662,7 @@ void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_m
 
 void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
     if (P.plane) return ns_plane_synthesize(P, c, x, st, analysis_masks);
+    if (P.slab) return ns_slab_synthesize(P, c, x, st, analysis_masks);
     const int es = P.nch;
     float2* A = P.acc.as<float2>();
     float2* K = P.comp.as<float2>();

@@ -128,10 +128,13 @@ __global__ void __launch_bounds__(256) ns_slab_mask_group_kernel(const float2* _
                                                                  BoxMap bx, NSMaskTables tb,
                                                                  const NSItem* __restrict__ items, int item0, int nz,
                                                                  int synth, float2* Y, long long ystride,
-                                                                 const float2* __restrict__ tw, int nlines) {
+                                                                 const float2* __restrict__ tw, int nlines,
+                                                                 long long xchs, long long ychs) {
     using Ge = RegGeom<N>;
     constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
     extern __shared__ float2 xch[];
+    X += blockIdx.z * xchs;   // channel
+    Y += blockIdx.z * ychs;
     const int tid = threadIdx.x;
     const int lp = tid % LP, p = tid / LP;
     const int l = blockIdx.x * LP + lp;
@@ -183,10 +186,13 @@ template <int N>
 __global__ void __launch_bounds__(256, 2) ns_slab_accum_kernel(const float2* __restrict__ Y, long long ystride, int G,
                                                             int P1, int s3, BoxMap bx, NSMaskTables tb,
                                                             const NSItem* __restrict__ items, int item0, int synth,
-                                                            float2* acc, const float2* __restrict__ tw, int nlines) {
+                                                            float2* acc, const float2* __restrict__ tw, int nlines,
+                                                            long long ychs, long long achs) {
     using Ge = RegGeom<N>;
     constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
     extern __shared__ float2 xch[];
+    Y += blockIdx.y * ychs;   // channel
+    acc += blockIdx.y * achs;
     const int tid = threadIdx.x;
     const int lp = tid % LP, p = tid / LP;
     const int l = blockIdx.x * LP + lp;
@@ -251,7 +257,9 @@ struct SlabArgs {
     float scale;             // applied to the C2R outputs
     int P1, n3;
     int nk1, nk2, b2;        // box: rows k1 < nk1, columns as BoxMap
-    int units;               // items x n3
+    int units;               // channels x items x n3
+    int nzc;                 // items a channel
+    long long spec_chstride; // spectra: channel stride (the volume's channels are interleaved floats)
     const float2* twa;       // w_n1^k, k < n1 (float64-designed)
     const float2* twb;       // w_n2^k, k < n2
     const float* tau;        // shrink pass: threshold of subband s at tau[s - 1]
@@ -354,8 +362,10 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
     const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
     const int k2hi = NB - (nk2 - b2 - 1);   // first negative-frequency column in the box
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
-        const int z = u / a.n3, s3 = u - z * a.n3;
-        const float2* src = a.spec + z * a.spec_zstride + (long long)s3 * SL;
+        const int per = a.nzc * a.n3;
+        const int ch = u / per, ur = u - ch * per;
+        const int z = ur / a.n3, s3 = ur - z * a.n3;
+        const float2* src = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         // 1. the box of the slab into shared memory
         for (int j = warp; j < nk2; j += kSlabWarps) {
             const int k2 = j <= b2 ? j : j + (NB - nk2);
@@ -391,7 +401,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
         {
             const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
             constexpr int npairs = NB / 2;
-            float* out = a.vol + a.vz.off(z) + (long long)s3 * PLANE * ES;
+            float* out = a.vol + ch + a.vz.off(z) + (long long)s3 * PLANE * ES;
             for (int base = 0; base < npairs; base += LA::LPR) {
                 if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
                 const int l = base + warp * LA::LPW + s;
@@ -455,12 +465,14 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
-        const int z = u / a.n3, s3 = u - z * a.n3;
+        const int per = a.nzc * a.n3;
+        const int ch = u / per, ur = u - ch * per;
+        const int z = ur / a.n3, s3 = ur - z * a.n3;
         // 1. R2C along axis 1 of columns 2l, 2l+1 (as the real and imaginary parts of one line)
         {
             const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
             constexpr int npairs = NB / 2;
-            const float* in = a.vol + a.vz.off(z) + (long long)s3 * PLANE * ES;
+            const float* in = a.vol + ch + a.vz.off(z) + (long long)s3 * PLANE * ES;
             for (int base = 0; base < npairs; base += LA::LPR) {
                 if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
                 const int l = base + warp * LA::LPW + s;
@@ -532,7 +544,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
         }
         __syncthreads();
         // 3. the box of the slab out to the spectrum
-        float2* dst = a.spec + z * a.spec_zstride + (long long)s3 * SL;
+        float2* dst = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         for (int j = warp; j < nk2; j += kSlabWarps) {
             const int k2 = j <= b2 ? j : j + (NB - nk2);
             for (int k1 = lane; k1 < nk1; k1 += 32) dst[k1 + P1 * k2] = S[k1 + P1 * k2];
@@ -566,8 +578,10 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_shrink_kernel(Slab
     const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
     const int k2hi = NB - (nk2 - b2 - 1);
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
-        const int z = u / a.n3, s3 = u - z * a.n3;
-        float2* slab = a.spec + z * a.spec_zstride + (long long)s3 * SL;
+        const int per = a.nzc * a.n3;
+        const int ch = u / per, ur = u - ch * per;
+        const int z = ur / a.n3, s3 = ur - z * a.n3;
+        float2* slab = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         const float tau = a.tau[a.items[a.item0 + z].s - 1];
         for (int j = warp; j < nk2; j += kSlabWarps) {
             const int k2 = j <= b2 ? j : j + (NB - nk2);
@@ -788,6 +802,8 @@ SlabArgs slab_args(const NSPlan& P, const NSBox& b, int nz) {
     a.nk2 = b.nk2;
     a.b2 = b.b2;
     a.units = nz * P.dims[2];
+    a.nzc = nz;
+    a.spec_chstride = 0;
     a.twa = P.ffts.at(P.dims[0])->sh.tw;
     a.twb = P.ffts.at(P.dims[1])->sh.tw;
     a.es = 1;
@@ -804,7 +820,7 @@ void line3(const NSPlan& P, const Load& ld, const Store& so, int nlines, int nz,
 
 template <int N>
 void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& bx, int i0, int synth, float2* acc,
-                       int nlines, cudaStream_t st) {
+                       int nlines, int nch, long long ychs, long long achs, cudaStream_t st) {
     using Ge = RegGeom<N>;
     static bool configured = false;
     if (!configured) {
@@ -813,18 +829,18 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    dim3 grid((nlines + Ge::LP - 1) / Ge::LP);
+    dim3 grid((nlines + Ge::LP - 1) / Ge::LP, nch);
     int tok = prof_begin("ns_slab_accum_axis3", st);
     ns_slab_accum_kernel<N><<<grid, Ge::THREADS, Ge::SMEM, st>>>(Y, P.SP, nz, P.P1, P.P1 * P.dims[1], bx, P.tb,
                                                                  P.items.as<NSItem>(), i0, synth, acc,
-                                                                 P.ffts.at(P.dims[2])->sh.tw, nlines);
+                                                                 P.ffts.at(P.dims[2])->sh.tw, nlines, ychs, achs);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
 }
 
 template <int N, int IPC>
 void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
-                           int nlines, cudaStream_t st) {
+                           int nlines, int nch, long long xchs, long long ychs, cudaStream_t st) {
     using Ge = RegGeom<N>;
     static bool configured = false;
     if (!configured) {
@@ -833,11 +849,11 @@ void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, 
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    dim3 grid((nlines + Ge::LP - 1) / Ge::LP, (nz + IPC - 1) / IPC);
+    dim3 grid((nlines + Ge::LP - 1) / Ge::LP, (nz + IPC - 1) / IPC, nch);
     int tok = prof_begin("ns_slab_mask_axis3", st);
     ns_slab_mask_group_kernel<N, IPC><<<grid, Ge::THREADS, Ge::SMEM, st>>>(
         X, P.P1, P.P1 * P.dims[1], bx, P.tb, P.items.as<NSItem>(), i0, nz, synth, Y, P.SP,
-        P.ffts.at(P.dims[2])->sh.tw, nlines);
+        P.ffts.at(P.dims[2])->sh.tw, nlines, xchs, ychs);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "ns_slab_mask_group_kernel launch");
 }
@@ -848,100 +864,113 @@ int mask_ipc(int nz) { return nz >= 4 ? 4 : (nz >= 2 ? 2 : 1); }
 
 template <int N>
 void launch_mask_group(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
-                       int nlines, cudaStream_t st) {
+                       int nlines, int nch, long long xchs, long long ychs, cudaStream_t st) {
     switch (mask_ipc(nz)) {
-        case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, st); return;
-        case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, st); return;
-        default: launch_mask_group_ipc<N, 1>(P, X, Y, nz, bx, i0, synth, nlines, st); return;
+        case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, st); return;
+        case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, st); return;
+        default: launch_mask_group_ipc<N, 1>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, st); return;
     }
 }
 
 // Algorithmic bytes of one box of a spectrum (complex float32 bins).
 double box_bytes(const NSPlan& P, const NSBox& b) { return 8.0 * b.nk1 * b.nk2 * P.dims[2]; }
 
-// rfft3 of one real channel (element stride es) into the padded spectrum X.
-void slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) {
+// Channels: complex volumes run their two real channels in the same launches
+// (spectra and intermediates one block per channel, the volume's channels
+// interleaved floats), with each channel's arithmetic that of a real volume.
+// Y blocks: channel ch of item z at work + ch * (group SP) + z * SP.
+long long ych_stride(const NSPlan& P) { return (long long)P.group * P.SP; }
+
+// rfft3 of nch interleaved real channels (element stride es) into the padded
+// spectra X + ch SP.
+void slab_rfft3(NSPlan& P, const float* x, int es, float2* X, int nch, cudaStream_t st) {
     const NSBox& full = P.boxes_full;
-    prof_bytes("ns_slab_r2c", 4.0 * P.N + box_bytes(P, full));
-    prof_bytes("ns_slab_line3", 2 * box_bytes(P, full));
+    prof_bytes("ns_slab_r2c", nch * (4.0 * P.N + box_bytes(P, full)));
+    prof_bytes("ns_slab_line3", nch * 2 * box_bytes(P, full));
     SlabArgs a = slab_args(P, full, 1);
+    a.units *= nch;
+    a.spec_chstride = P.SP;
     a.spec = X;
     a.vol = const_cast<float*>(x);
     a.es = es;
-    launch_slab<0>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
-                       "ns_slab_r2c");
+    launch_slab<0>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_r2c");
     const BoxMap bx = box_map(P, full);
     const int s3 = P.P1 * P.dims[1];
-    line3<false>(P, L3LoadC{X, 0, P.P1, s3, bx}, L3StoreC{X, 0, P.P1, s3, bx}, full.nk1 * full.nk2, 1, st,
+    line3<false>(P, L3LoadC{X, P.SP, P.P1, s3, bx}, L3StoreC{X, P.SP, P.P1, s3, bx}, full.nk1 * full.nk2, nch, st,
                  "ns_slab_line3");
 }
 
-// irfft3 of the padded spectrum A (overwritten) into one real channel.
-void slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) {
+// irfft3 of the padded spectra A + ch SP (overwritten) into nch channels.
+void slab_irfft3(NSPlan& P, float2* A, float* x, int es, int nch, cudaStream_t st) {
     const NSBox& full = P.boxes_full;
-    prof_bytes("ns_slab_line3", 2 * box_bytes(P, full));
-    prof_bytes("ns_slab_c2r", box_bytes(P, full) + 4.0 * P.N);
+    prof_bytes("ns_slab_line3", nch * 2 * box_bytes(P, full));
+    prof_bytes("ns_slab_c2r", nch * (box_bytes(P, full) + 4.0 * P.N));
     const BoxMap bx = box_map(P, full);
     const int s3 = P.P1 * P.dims[1];
-    line3<true>(P, L3LoadC{A, 0, P.P1, s3, bx}, L3StoreC{A, 0, P.P1, s3, bx}, full.nk1 * full.nk2, 1, st,
+    line3<true>(P, L3LoadC{A, P.SP, P.P1, s3, bx}, L3StoreC{A, P.SP, P.P1, s3, bx}, full.nk1 * full.nk2, nch, st,
                 "ns_slab_line3");
     SlabArgs a = slab_args(P, full, 1);
+    a.units *= nch;
+    a.spec_chstride = P.SP;
     a.spec = A;
     a.vol = x;
     a.es = es;
     a.scale = 1.0f / (float)P.N;
-    launch_slab<1>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st,
-                      "ns_slab_c2r");
+    launch_slab<1>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_c2r");
 }
 
 // The analysis axis-3 pass of items [i0, i0 + nz) (one mask group): X times
 // each mask, inverse FFT along axis 3, into Y (the plan's work spectra).
-void slab_mask_pass(NSPlan& P, const float2* X, int i0, int nz, bool synth_masks, cudaStream_t st) {
+void slab_mask_pass(NSPlan& P, const float2* X, int i0, int nz, bool synth_masks, int nch, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     const BoxMap bx = box_map(P, b);
     float2* Y = P.work.as<float2>();
-    prof_bytes("ns_slab_mask_axis3", 1.5 * box_bytes(P, b) + nz * box_bytes(P, b));
+    prof_bytes("ns_slab_mask_axis3", nch * (1.5 * box_bytes(P, b) + nz * box_bytes(P, b)));
     const int nl = b.nk1 * b.nk2, sy = synth_masks ? 1 : 0;
+    const long long xc = P.SP, yc = ych_stride(P);
     switch (P.dims[2]) {
-        case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, st); return;
-        case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, st); return;
-        case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, st); return;
-        case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, st); return;
-        case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, st); return;
-        case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, st); return;
-        case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, st); return;
+        case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
     }
     throw ArgError("no register line pass for axis 3 of this size");
 }
 
-// The synthesis axis-3 pass of items [i0, i0 + nz) from Y into acc.
-void slab_accum_pass(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, cudaStream_t st) {
+// The synthesis axis-3 pass of items [i0, i0 + nz) from Y into acc + ch SP.
+void slab_accum_pass(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, int nch, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     const float2* Y = P.work.as<float2>();
-    prof_bytes("ns_slab_accum_axis3", nz * box_bytes(P, b) + 0.5 * box_bytes(P, b) + 2 * box_bytes(P, b));
+    prof_bytes("ns_slab_accum_axis3", nch * (nz * box_bytes(P, b) + 0.5 * box_bytes(P, b) + 2 * box_bytes(P, b)));
     const BoxMap bx = box_map(P, b);
     const int nl = b.nk1 * b.nk2;
     const int sy = analysis_masks ? 0 : 1;
+    const long long yc = ych_stride(P), ac = P.SP;
     switch (P.dims[2]) {
-        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
-        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
-        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
-        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
-        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
-        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
-        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, nl, st); return;
+        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
     }
     throw ArgError("no register line pass for axis 3 of this size");
 }
 
-// Analysis of items [i0, i0 + nz) (one mask group) from X into volumes at
-// vol + vz.off(z).
+// Analysis of items [i0, i0 + nz) (one mask group) from X (+ ch SP) into
+// volumes at vol + vz.off(z) (+ ch, element stride es).
 void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
-                        cudaStream_t st) {
+                        int nch, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
-    slab_mask_pass(P, X, i0, nz, synth_masks, st);
-    prof_bytes("ns_slab_c2r", nz * (box_bytes(P, b) + 4.0 * P.N));
+    slab_mask_pass(P, X, i0, nz, synth_masks, nch, st);
+    prof_bytes("ns_slab_c2r", nch * nz * (box_bytes(P, b) + 4.0 * P.N));
     SlabArgs a = slab_args(P, b, nz);
+    a.units *= nch;
+    a.spec_chstride = ych_stride(P);
     a.spec = P.work.as<float2>();
     a.spec_zstride = P.SP;
     a.vol = vol;
@@ -952,27 +981,30 @@ void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es,
 }
 
 // Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
-// vol + vz.off(z) into acc.
+// vol + vz.off(z) (+ ch) into acc + ch SP.
 void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
-                      float2* acc, cudaStream_t st) {
+                      float2* acc, int nch, cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
-    prof_bytes("ns_slab_r2c", nz * (4.0 * P.N + box_bytes(P, b)));
+    prof_bytes("ns_slab_r2c", nch * nz * (4.0 * P.N + box_bytes(P, b)));
     SlabArgs a = slab_args(P, b, nz);
+    a.units *= nch;
+    a.spec_chstride = ych_stride(P);
     a.spec = P.work.as<float2>();
     a.spec_zstride = P.SP;
     a.vol = const_cast<float*>(vol);
     a.vz = vz;
     a.es = es;
     launch_slab<0>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_r2c");
-    slab_accum_pass(P, i0, nz, analysis_masks, acc, st);
+    slab_accum_pass(P, i0, nz, analysis_masks, acc, nch, st);
 }
 
-// The denoiser on items [i0, i0 + nz) (one mask group): the analysis axis-3
-// pass into Y, the shrink slab pass in place, the synthesis accumulation.
+// The denoiser on items [i0, i0 + nz) (one mask group; real data): the
+// analysis axis-3 pass into Y, the shrink slab pass in place, the synthesis
+// accumulation.
 void slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
                         cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
-    slab_mask_pass(P, X, i0, nz, false, st);
+    slab_mask_pass(P, X, i0, nz, false, 1, st);
     prof_bytes("ns_slab_shrink", nz * 2 * box_bytes(P, b));
     SlabArgs a = slab_args(P, b, nz);
     a.spec = P.work.as<float2>();
@@ -982,7 +1014,7 @@ void slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float*
     a.items = P.items.as<NSItem>();
     a.item0 = i0;
     launch_slab<2>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_shrink");
-    slab_accum_pass(P, i0, nz, false, acc, st);
+    slab_accum_pass(P, i0, nz, false, acc, 1, st);
 }
 
 // Consecutive items of one mask group, at most P.group of them.
@@ -1037,20 +1069,44 @@ void ns_use_slabs(NSPlan& P) {
     ns_alloc_scratch(P);
 }
 
-void ns_slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) { slab_rfft3(P, x, es, X, st); }
+void ns_slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st) { slab_rfft3(P, x, es, X, 1, st); }
 
-void ns_slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) { slab_irfft3(P, A, x, es, st); }
+void ns_slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) { slab_irfft3(P, A, x, es, 1, st); }
+
+// Whole transforms, both channels of complex data in every launch.
+void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
+    const int nch = P.nch;
+    float2* X = P.X.as<float2>();
+    slab_rfft3(P, static_cast<const float*>(x), nch, X, nch, st);
+    for (int i0 = 0, i1; i0 < P.S; i0 = i1) {
+        i1 = chunk_end(P, i0);
+        slab_analyze_items(P, X, static_cast<float*>(c), ns_subband_map(P, i0, nch), nch, i0, i1 - i0, synth_masks,
+                           nch, st);
+    }
+}
+
+void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
+    const int nch = P.nch;
+    float2* A = P.acc.as<float2>();
+    cuda_check(cudaMemsetAsync(A, 0, sizeof(float2) * P.SP * nch, st), "cudaMemsetAsync(acc)");
+    for (int i0 = 0, i1; i0 < P.S; i0 = i1) {
+        i1 = chunk_end(P, i0);
+        slab_synth_items(P, static_cast<const float*>(c), ns_subband_map(P, i0, nch), nch, i0, i1 - i0,
+                         analysis_masks, A, nch, st);
+    }
+    slab_irfft3(P, A, static_cast<float*>(x), nch, nch, st);
+}
 
 int ns_slab_chunk_end(const NSPlan& P, int i0) { return chunk_end(P, i0); }
 
 void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
                            cudaStream_t st) {
-    slab_analyze_items(P, X, vol, vz, es, i0, nz, synth_masks, st);
+    slab_analyze_items(P, X, vol, vz, es, i0, nz, synth_masks, 1, st);
 }
 
 void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
                          float2* acc, cudaStream_t st) {
-    slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, st);
+    slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, 1, st);
 }
 
 void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,

@@ -171,6 +171,8 @@ NSBox ns_make_box(int nk1, int b2, int n2);
 NSBox ns_table_box(const std::vector<double>& g, int h1, int n2, int n3);
 void ns_alloc_scratch(NSPlan& P);
 void ns_slab_rfft3(NSPlan& P, const float* x, int es, float2* X, cudaStream_t st);
+void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
+void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
 void ns_slab_irfft3(NSPlan& P, float2* A, float* x, int es, cudaStream_t st);
 int ns_slab_chunk_end(const NSPlan& P, int i0);
 void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
