@@ -449,6 +449,46 @@ def main():
                             "three_calls_value": B * N / (ms_three / 1e3) / 1e6, "unit": "Mvoxels/s",
                             "equal_bit_for_bit": bool(torch.equal(yn, ys[B - 1]))}
 
+        # batch workload: 64 volumes, axes from {64, 96, 128, 160}, scales from {2, 3, 4},
+        # levels from {1, 2, 3}; analyze + synthesize + adjoint as one graph against a loop
+        brng = np.random.default_rng(64)
+        bws, bx, bc, by, nvox = [], [], [], [], 0
+        t0 = time.perf_counter()
+        for _ in range(64):
+            d3 = tuple(int(v) for v in brng.choice([64, 96, 128, 160], 3))
+            J = int(brng.choice([2, 3, 4]))
+            w = sfl.make_workspace(sfl.NSSurfacelet(scales=J, direction_levels=[int(v) for v in brng.choice([1, 2, 3], J)]),
+                                   "float32", d3)
+            xv = sfl.volume_like(d3).copy_(torch.randn(d3, device="cuda"))
+            w.autotune(xv)
+            bws.append(w)
+            bx.append(xv)
+            bc.append(sfl.similar_coefficients(w.transform, xv))
+            by.append(sfl.volume_like(d3))
+            nvox += int(np.prod(d3))
+        t_setup = time.perf_counter() - t0
+        bents = []
+        for w, xv, cv, yv in zip(bws, bx, bc, by):
+            bents += [(w, "analyze", xv, cv), (w, "synthesize", cv, yv), (w, "adjoint_synthesize", yv, cv)]
+        bb = sfl.Batch([e[0] for e in bents], [e[2] for e in bents], [e[3] for e in bents], [e[1] for e in bents])
+
+        def loop_step():
+            for w, xv, cv, yv in zip(bws, bx, bc, by):
+                sfl.analyze_(cv, w, xv)
+                sfl.synthesize_(yv, w, cv)
+                sfl.adjoint_synthesize_(cv, w, yv)
+
+        loop_step()
+        ms_graph = timed(bb.run, 3)
+        ms_loop = timed(loop_step, 3)
+        line["batch64"] = {"workload": "64 NSSurfacelet volumes, axes from {64,96,128,160}, scales from {2,3,4}, "
+                                       "levels from {1,2,3} (seed 64), analyze+synthesize+adjoint, autotuned plans",
+                           "graph_value": nvox / (ms_graph / 1e3) / 1e6, "loop_value": nvox / (ms_loop / 1e3) / 1e6,
+                           "unit": "Mvoxels/s", "voxels": nvox, "setup_s": t_setup}
+        bb.close()
+        del bb, bws, bx, bc, by
+        torch.cuda.empty_cache()
+
         # CPU baseline: the oracle port on the host cores, bounded sample
         from oracle.cpu_baseline import NSBaseline
         cores = os.cpu_count()

@@ -190,6 +190,17 @@ int sfl_plan_set_group(sfl_plan* plan, int32_t group);
 #define SFL_PIPELINE_SLABS 2
 int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline);
 
+/* The plan's pipeline and group.  No counterpart in the reference. */
+int sfl_plan_tuning(const sfl_plan* plan, int32_t* pipeline, int32_t* group);
+
+/* Times analysis of x (into c, overwritten) under every pipeline that fits
+ * the size and groups of 2, 4 and 8 subbands, keeps the fastest, and records
+ * it for the process: NS and NDFB plans created later with the same
+ * transform, size and element type start with it.  Synchronizes; reallocates
+ * the plan's scratch.  No-op for decimated plans.  No counterpart in the
+ * reference (its plans are FFTW-tuned instead). */
+int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream);
+
 /* ── Transforms ─────────────────────────────────────────────────────────── */
 
 /* analyze!(c, t, x; workspace): src/transforms/ns_surfacelet.jl:551-566,

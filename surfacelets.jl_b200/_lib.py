@@ -85,6 +85,8 @@ SIGNATURES = {
     "sfl_subband_info": (C.c_int, [P, C.c_int32, Dims, C.POINTER(C.c_int64)]),
     "sfl_plan_set_group": (C.c_int, [P, C.c_int32]),
     "sfl_plan_set_pipeline": (C.c_int, [P, C.c_int32]),
+    "sfl_plan_tuning": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "sfl_plan_autotune": (C.c_int, [P, P, P, P]),
     "sfl_plan_status": (C.c_int, [P, C.POINTER(C.c_int32), C.c_int32]),
     "sfl_analyze": (C.c_int, [P, P, P, P]),
     "sfl_synthesize": (C.c_int, [P, P, P, P]),

@@ -6,6 +6,8 @@
 
 #include <cstring>
 #include <memory>
+#include <mutex>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -109,6 +111,59 @@ void on_device(const sfl_plan* plan, F&& f) {
         throw;
     }
     if (cur != plan->impl.device) sfl::cuda_check(cudaSetDevice(cur), "cudaSetDevice");
+}
+
+// Pipeline and group of an NS plan (the two knobs of the tuner).
+void ns_apply(sfl::NSPlan& N, int pipeline, int group) {
+    cudaDeviceSynchronize();
+    if (pipeline == SFL_PIPELINE_LINES) {
+        N.plane = false;
+        if (N.slab) {
+            N.slab = false;
+            sfl::ns_alloc_scratch(N);
+        }
+    } else if (pipeline == SFL_PIPELINE_PLANES) {
+        sfl::ns_use_planes(N);
+    } else if (pipeline == SFL_PIPELINE_SLABS) {
+        sfl::ns_use_slabs(N);
+    } else {
+        throw sfl::ArgError("unknown pipeline " + std::to_string(pipeline));
+    }
+    if (group >= 1 && std::min(group, N.S) != N.group) {
+        N.group = std::min(group, N.S);
+        sfl::ns_alloc_scratch(N);
+    }
+}
+
+int ns_pipeline_of(const sfl::NSPlan& N) {
+    return N.slab ? SFL_PIPELINE_SLABS : (N.plane ? SFL_PIPELINE_PLANES : SFL_PIPELINE_LINES);
+}
+
+// Tuned (pipeline, group) per transform, size and element type, for the
+// lifetime of the process; plans created later with the same key start tuned.
+std::mutex g_tuned_mu;
+std::map<std::string, std::pair<int, int>> g_tuned;
+
+std::string tune_key(const sfl::NSPlan& N, int dtype) {
+    std::string k = (N.ndfb ? "ndfb" : "ns") + std::string(":");
+    for (int i = 0; i < 3; ++i) k += std::to_string(N.dims[i]) + ",";
+    k += std::to_string(dtype) + ":" + std::to_string(N.p.scales) + ":";
+    for (int j = 0; j < N.p.scales; ++j) k += std::to_string(N.p.direction_levels[j]) + ",";
+    k += ":" + std::to_string(N.p.bernstein_order) + ":" + std::to_string(N.p.halfband_order) + ":" +
+         std::to_string(N.p.transition) + ":" + std::to_string(N.p.tight);
+    return k;
+}
+
+void apply_tuned(sfl_plan* plan) {
+    sfl::NSPlan& N = *plan->impl.ns;
+    std::pair<int, int> t;
+    {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        auto it = g_tuned.find(tune_key(N, plan->impl.dtype));
+        if (it == g_tuned.end()) return;
+        t = it->second;
+    }
+    ns_apply(N, t.first, t.second);
 }
 
 // One transform of a plan (the four operators of the C ABI).
@@ -289,6 +344,7 @@ int sfl_ns_plan_create(const sfl_ns_params* p, const int32_t dims[3], int32_t dt
         sfl::cuda_check(cudaGetDevice(&plan->impl.device), "cudaGetDevice");
         plan->impl.ns.reset(new sfl::NSPlan);
         sfl::ns_plan_init(*plan->impl.ns, *p, d, dtype);
+        apply_tuned(plan.get());
         *out = plan.release();
         return SFL_OK;
     });
@@ -333,6 +389,7 @@ int sfl_ndfb_plan_create(const sfl_ndfb_params* p, const int32_t dims[3], int32_
         sfl::cuda_check(cudaGetDevice(&plan->impl.device), "cudaGetDevice");
         plan->impl.ns.reset(new sfl::NSPlan);
         sfl::ns_plan_init(*plan->impl.ns, q, d, dtype, true);
+        apply_tuned(plan.get());
         *out = plan.release();
         return SFL_OK;
     });
@@ -463,21 +520,73 @@ int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline) {
         if (plan->impl.kind != SFL_KIND_NS) throw sfl::ArgError("pipeline selection applies to NSSurfacelet plans");
         sfl::NSPlan& N = *plan->impl.ns;
         if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+        on_device(plan, [&] { ns_apply(N, pipeline, 0); });
+        return SFL_OK;
+    });
+}
+
+int sfl_plan_tuning(const sfl_plan* plan, int32_t* pipeline, int32_t* group) {
+    return guarded([&] {
+        need(plan, "plan");
+        if (plan->impl.kind != SFL_KIND_NS) {
+            if (pipeline) *pipeline = -1;
+            if (group) *group = 0;
+            return SFL_OK;
+        }
+        const sfl::NSPlan& N = *plan->impl.ns;
+        if (pipeline) *pipeline = ns_pipeline_of(N);
+        if (group) *group = N.group;
+        return SFL_OK;
+    });
+}
+
+int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(x, "x");
+        need(c, "c");
+        if (plan->impl.kind != SFL_KIND_NS) return SFL_OK;   // the decimated transform has no knobs
+        sfl::NSPlan& N = *plan->impl.ns;
+        if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
+        check_aligned(x, plan->impl.dtype, "x");
+        check_aligned(c, plan->impl.dtype, "c");
         on_device(plan, [&] {
-            cudaDeviceSynchronize();
-            if (pipeline == SFL_PIPELINE_LINES) {
-                N.plane = false;
-                if (N.slab) {
-                    N.slab = false;
-                    sfl::ns_alloc_scratch(N);
-                }
-            } else if (pipeline == SFL_PIPELINE_PLANES) {
-                sfl::ns_use_planes(N);
-            } else if (pipeline == SFL_PIPELINE_SLABS) {
-                sfl::ns_use_slabs(N);
+            cudaStream_t st = as_stream(stream);
+            std::vector<int> pipes;
+            if (sfl::ns_slab_supported(N.dims[0], N.dims[1], N.dims[2])) pipes.push_back(SFL_PIPELINE_SLABS);
+            pipes.push_back(SFL_PIPELINE_LINES);
+            cudaEvent_t e0, e1;
+            sfl::cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+            sfl::cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+            float best = 1e30f;
+            std::pair<int, int> pick{ns_pipeline_of(N), N.group};
+            try {
+                for (int pipe : pipes)
+                    for (int g : {2, 4, 8}) {
+                        if (g > N.S && g != 2) continue;
+                        ns_apply(N, pipe, g);
+                        sfl::ns_analyze(N, x, c, st, false);   // warm-up
+                        sfl::cuda_check(cudaEventRecord(e0, st), "cudaEventRecord");
+                        for (int r = 0; r < 2; ++r) sfl::ns_analyze(N, x, c, st, false);
+                        sfl::cuda_check(cudaEventRecord(e1, st), "cudaEventRecord");
+                        sfl::cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+                        float ms = 0;
+                        sfl::cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                        if (ms < best) {
+                            best = ms;
+                            pick = {pipe, g};
+                        }
+                    }
+            } catch (...) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                throw;
             }
-            else
-                throw sfl::ArgError("unknown pipeline " + std::to_string(pipeline));
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            ns_apply(N, pick.first, pick.second);
+            std::lock_guard<std::mutex> lk(g_tuned_mu);
+            g_tuned[tune_key(N, plan->impl.dtype)] = pick;
         });
         return SFL_OK;
     });

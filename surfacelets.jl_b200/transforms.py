@@ -425,6 +425,26 @@ class Workspace:
 
     PIPELINES = {"lines": 0, "planes": 1, "slabs": 2}
 
+    def tuning(self):
+        """(pipeline name, group) in use."""
+        pi, g = C.c_int32(), C.c_int32()
+        check(lib.sfl_plan_tuning(self._h, C.byref(pi), C.byref(g)))
+        names = {v: k for k, v in self.PIPELINES.items()}
+        return names.get(pi.value), g.value
+
+    def autotune(self, x=None, stream=None):
+        """Time analysis under each pipeline and group size, keep the fastest and
+        remember it for later workspaces of the same transform, size and type.
+        x: a device volume to time on (random when omitted)."""
+        if not isinstance(self.transform, NSSurfacelet):
+            return self.tuning()
+        if x is None:
+            x = volume_like(self.dims, "complex64" if self.dtype else "float32")
+            x.copy_(torch.randn(x.shape, dtype=x.dtype, device=x.device))
+        c = similar_coefficients(self.transform, x)
+        check(lib.sfl_plan_autotune(self._h, _ptr(x), _ptr(c), _stream(stream)))
+        return self.tuning()
+
     def set_pipeline(self, name):
         """NSSurfacelet kernel pipeline: "slabs" (the default where the size
         allows), "lines" or "planes"."""

@@ -3,7 +3,8 @@ oracle (test infrastructure):
 
     L(c) = 0.5 || M o FFT3(synthesize(c)) - y ||^2 + lam sum sqrt(|c|^2 + eps^2)
 
-M a seeded Bernoulli(0.25) mask, y = M o FFT3(phantom), lam = 1e-3,
+M a seeded Bernoulli(0.25) k-space mask with a fully sampled 16^3 centre
+(DC-centred, wrap-around indexing), y = M o FFT3(phantom), lam = 1e-3,
 eps = 1e-6.  Complex volumes and coefficients go through the real oracle
 channel by channel; gradients pack d/dRe + i d/dIm."""
 
@@ -48,6 +49,8 @@ def make_problem(dims, seed):
     ph = ellipsoid_phantom(dims, seed=seed).astype(np.float64)
     ph = ph + 1j * ellipsoid_phantom(dims, seed=seed + 1)
     M = (rng.random(dims) < 0.25).astype(np.float64)
+    c = [np.r_[0:min(8, n), max(n - 8, min(8, n)):n] for n in dims]   # |k| < 8 on every axis, wrapped
+    M[np.ix_(*c)] = 1.0
     y = M * np.fft.fftn(ph)
     return ph, M, y, rng
 

@@ -115,3 +115,56 @@ def test_batch_copies_volumes_to_and_from_pinned_host_memory(sfl):
     with pytest.raises(sfl.ArgumentError):
         sfl.Batch([wss[0]], [torch.empty(wss[0].dims[::-1])], [sfl.volume_like(wss[0].dims)], ["copy_volume"])
     b.close()
+
+
+def _mixed_configs(n, seed):
+    # the batch workload: every axis from {64, 96, 128, 160}, scales from {2, 3, 4},
+    # each scale's direction level from {1, 2, 3}
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        dims = tuple(int(v) for v in rng.choice([64, 96, 128, 160], 3))
+        J = int(rng.choice([2, 3, 4]))
+        out.append((dims, dict(scales=J, direction_levels=[int(v) for v in rng.choice([1, 2, 3], J)])))
+    return out
+
+
+def test_autotune_picks_and_remembers(sfl):
+    dims = (64, 96, 64)
+    t = sfl.NSSurfacelet(scales=3, direction_levels=[2, 1, 3])
+    ws = sfl.make_workspace(t, "float32", dims)
+    x = sfl.to_device(np.random.default_rng(2).standard_normal(dims).astype(np.float32))
+    c0 = sfl.analyze(ws, x)
+    pick = ws.autotune(x)
+    assert pick[0] in ("slabs", "lines") and pick[1] in (2, 4, 8)
+    c1 = sfl.analyze(ws, x)
+    assert float(torch.linalg.vector_norm(c1 - c0) / torch.linalg.vector_norm(c0)) <= 1e-6
+    assert sfl.make_workspace(t, "float32", dims).tuning() == pick          # the process-wide record
+    assert sfl.make_workspace(t, "complex64", dims).tuning()[1] == 8        # another element type: untuned
+
+
+def test_mixed_batch_as_one_graph(sfl):
+    cfgs = _mixed_configs(8, 44)
+    rng = np.random.default_rng(45)
+    wss, xs = [], []
+    for dims, kw in cfgs:
+        ws = sfl.make_workspace(sfl.NSSurfacelet(**kw), "float32", dims)
+        x = sfl.to_device(rng.standard_normal(dims).astype(np.float32))
+        ws.autotune(x)
+        wss.append(ws)
+        xs.append(x)
+    cs = [_coef(sfl, ws) for ws in wss]
+    ys = [sfl.volume_like(ws.dims) for ws in wss]
+    gs = [_coef(sfl, ws) for ws in wss]
+    ents = []
+    for ws, x, c, y, g in zip(wss, xs, cs, ys, gs):
+        ents += [(ws, "analyze", x, c), (ws, "synthesize", c, y), (ws, "adjoint_synthesize", y, g)]
+    b = sfl.Batch([e[0] for e in ents], [e[2] for e in ents], [e[3] for e in ents], [e[1] for e in ents])
+    b.run()
+    torch.cuda.synchronize()
+    for ws, x, c, y, g in zip(wss, xs, cs, ys, gs):
+        c0 = sfl.analyze(ws, x)
+        assert torch.equal(c, c0)
+        assert torch.equal(y, sfl.synthesize(ws, c0))
+        assert float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x)) <= 1e-5
+    b.close()

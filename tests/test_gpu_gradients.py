@@ -3,7 +3,8 @@ compressed-sensing loss of the complex workload
 
     L(c) = 0.5 || M o FFT3(synthesize(c)) - y ||^2 + lam sum sqrt(|c|^2 + eps^2)
 
-with M a seeded Bernoulli(0.25) sampling mask and y = M o FFT3(phantom):
+with M a seeded Bernoulli(0.25) sampling mask with a fully sampled 16^3 centre
+and y = M o FFT3(phantom):
 the device gradient is held against the float64 oracle gradient (itself
 pinned by central differences in test_oracle_gradients.py), and the same for
 the gradient through analyze, x -> L(analyze(x)).  At 128^3 the device

@@ -178,3 +178,18 @@ def test_adjoints_at_128_mode_2_and_complex_linearity(sfl):
     zr = sfl.to_host(sfl.adjoint_analyze(wr, torch.from_numpy(cr).cuda(), dims=dz))
     zi = sfl.to_host(sfl.adjoint_analyze(wr, torch.from_numpy(ci).cuda(), dims=dz))
     assert np.array_equal(zc.real, zr) and np.array_equal(zc.imag, zi)
+
+
+@pytest.mark.parametrize("dims,mode,red", [((128, 128, 128), 2, 3.4238), ((96, 96, 96), 1.5, 4.0046)])
+def test_phantom_workload_against_oracle(sfl, dims, mode, red):
+    # the decimated workload: Surfacelet(scales=3, direction_levels=[2,2,3]) on the
+    # 12-ellipsoid phantom plus N(0, 0.05^2) noise, about 3.4 / 4 coefficients a voxel
+    from phantoms import ellipsoid_phantom
+    x = ellipsoid_phantom(dims, count=12, seed=21, noise=0.05)
+    t = sfl.Surfacelet(scales=3, direction_levels=[2, 2, 3], pyramid_ratio=mode)
+    assert abs(sfl.surfacelet_redundancy(t, dims) - red) < 1e-4
+    T = D.make_tables(D.SurfParams.make(scales=3, direction_levels=[2, 2, 3], pyramid_ratio=mode), dims)
+    ws = sfl.make_workspace(t, "float32", dims)
+    c = sfl.analyze(ws, sfl.to_device(x))
+    assert rel_l2(c.cpu().numpy(), D.analyze(T, x.astype(np.float64))) <= REL
+    assert rel_l2(sfl.to_host(sfl.synthesize(ws, c)), x) <= REL
