@@ -261,7 +261,10 @@ int sfl_ns_analyze_subband_static(sfl_plan* plan, const void* x, void* band, int
  * transform on `dims` to out (when not NULL) and its element count to *count.
  * Names (NS): "m1", "m2", "wedge" (index = ((scale-1)*3 + hourglass-1)*64*2
  * + plane*64 + wedge-1, plane 0 = a, 1 = b), "pa" (index = level*3 + axis),
- * "pl" (same).  Names (decimated): "ritf" (index = level*3 + K-1),
+ * "pl" (same), "group" (B_j times the hourglass factor of a plan's group
+ * table; index = (scale-1)*3 + hourglass-1), "bandpass" (B_j; index = level,
+ * 0 = finest), "hourglass" (the standalone bank's mask; index = hourglass-1).
+ * Names (decimated): "ritf" (index = level*3 + K-1),
  * "irc" (complex as re/im pairs; index = ((level*3 + K-1)*32 + stage)*4 + which,
  * which 0,1 = analysis channel 0,1 and 2,3 = synthesis channel 0,1),
  * "pyr_prof" (index = level*3 + axis).  No counterpart in the reference's
@@ -270,6 +273,12 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
                         int32_t index, double* out, int64_t* count);
 int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name,
                           int32_t index, double* out, int64_t* count);
+/* The float32 tables an NSSurfacelet or NDFB plan holds on the device (designed
+ * there in float64): "group" (index = (scale-1)*3 + hourglass-1) and, for an
+ * untight plan, "bandpass" (index = level, 0 = finest).  Writes H = (n1/2+1)
+ * n2 n3 floats to the host buffer out (when not NULL) and H to *count.
+ * Equal bit for bit to the float64 host design rounded to float32. */
+int sfl_ns_plan_table(sfl_plan* plan, const char* name, int32_t index, float* out, int64_t* count);
 
 /* ── Soft-threshold denoiser (NSSurfacelet and NDFB plans, Float32) ─────
  * No counterpart in the reference.  y = synthesize(soft(analyze(x), tau)),

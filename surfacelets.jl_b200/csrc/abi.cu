@@ -747,6 +747,7 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
         dims_of(dims, d);
         sfl::NSDesign D = sfl::ns_design(*p, d);
         const std::vector<double>* v = nullptr;
+        std::vector<double> tmp;
         std::string nm(name);
         if (nm == "m1") {
             v = &D.m1;
@@ -758,6 +759,19 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
             const sfl::WedgePlanes& W = D.wedges[j][hi][plane];
             if (w >= (int)W.w.size()) throw sfl::ArgError("wedge table index out of range");
             v = &W.w[w];
+        } else if (nm == "group") {
+            // plan order: g = 3 (scale - 1) + hourglass - 1
+            if (index < 0 || index >= 3 * p->scales) throw sfl::ArgError("group index out of range");
+            tmp = sfl::ns_group_mask(D, p->scales - 1 - index / 3, index % 3 + 1, true);
+            v = &tmp;
+        } else if (nm == "bandpass") {
+            if (index < 0 || index >= p->scales) throw sfl::ArgError("level out of range");
+            tmp = sfl::ns_group_mask(D, index, 1, false);
+            v = &tmp;
+        } else if (nm == "hourglass") {
+            if (index < 0 || index >= 3) throw sfl::ArgError("hourglass index out of range");
+            tmp = sfl::ns_hourglass_mask(D, index + 1);
+            v = &tmp;
         } else if (nm == "pa" || nm == "pl") {
             int lv = index / 3, ax = index % 3;
             auto& tab = nm == "pa" ? D.pa : D.pl;
@@ -768,6 +782,35 @@ int sfl_ns_design_table(const sfl_ns_params* p, const int32_t dims[3], const cha
         }
         *count = (int64_t)v->size();
         if (out) std::memcpy(out, v->data(), sizeof(double) * v->size());
+        return SFL_OK;
+    });
+}
+
+int sfl_ns_plan_table(sfl_plan* plan, const char* name, int32_t index, float* out, int64_t* count) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan);
+        need(name, "name");
+        need(count, "count");
+        std::string nm(name);
+        const sfl::DevMem* m = nullptr;
+        int n = 0;
+        if (nm == "group") {
+            m = &N.G;
+            n = N.ndfb ? 3 : 3 * N.p.scales;
+        } else if (nm == "bandpass") {
+            m = &N.Bl;
+            n = N.p.tight ? 0 : (N.ndfb ? 1 : N.p.scales);
+        } else {
+            throw sfl::ArgError("unknown table " + nm);
+        }
+        if (index < 0 || index >= n) throw sfl::ArgError("table index out of range");
+        *count = N.H;
+        if (out)
+            on_device(plan, [&] {
+                sfl::cuda_check(cudaMemcpy(out, m->as<float>() + (size_t)index * N.H, sizeof(float) * N.H,
+                                           cudaMemcpyDeviceToHost),
+                                "table readback");
+            });
         return SFL_OK;
     });
 }

@@ -120,18 +120,23 @@ std::vector<double> bernstein_table(int N, const std::vector<double>& omega) {
     return tbl;
 }
 
-// src/filters/bernstein.jl:171-190 — the sum first, scaled last.
+// src/filters/bernstein.jl:171-190 — the sum first, scaled last.  The powers
+// are running products, so the device-side design (ns_design.cu) repeats the
+// same roundings.
 double halfband_split(double x, int m) {
     if (m < 0) throw ArgError("polynomial order must be ≥ 0");
     double u = (1 + x) / 2;
     double v = (1 - x) / 2;
     if (u == 0) return 0.0;
-    double s = 0, c = 1;
+    double s = 0, c = 1, vk = 1;
     for (int k = 0; k <= m; ++k) {
-        s += c * std::pow(v, k);
+        s += c * vk;
         c = c * (m + k + 1) / (k + 1);
+        vk *= v;
     }
-    return std::pow(u, m + 1) * s;
+    double um = 1;
+    for (int k = 0; k <= m; ++k) um *= u;
+    return um * s;
 }
 
 // src/filters/bernstein.jl:196-203
@@ -293,45 +298,32 @@ static WedgePlanes wedge_masks_plane(const int dims[3], int ref, int tr, int l, 
 }
 
 // src/directional/hourglass.jl:172-189 and src/filters/bernstein.jl:97-151
-static void hourglass_tables(const int dims[3], int order, int poly, std::vector<double>& m1,
-                             std::vector<double>& m2) {
+// The separable parts of the hourglass tables (src/directional/hourglass.jl:
+// 172-189): the Bernstein tables of axes 2 and 3, the 3-D mapping kernel
+// contracted along axis 1, t1[j2, j3, k1], and m2 = f0(M2) on (n2, n3).
+NSHourglassFactors ns_hourglass_factors(const int dims[3], int order, int poly) {
+    NSHourglassFactors F;
     int n1 = dims[0], n2 = dims[1], n3 = dims[2], h1 = n1 / 2 + 1;
     int np = order + 1;
+    F.np = np;
     std::vector<double> b1 = bernstein_table(order, dft_frequencies(n1, true));
-    std::vector<double> b2 = bernstein_table(order, dft_frequencies(n2, false));
-    std::vector<double> b3 = bernstein_table(order, dft_frequencies(n3, false));
+    F.b2 = bernstein_table(order, dft_frequencies(n2, false));
+    F.b3 = bernstein_table(order, dft_frequencies(n3, false));
+    const std::vector<double>& b2 = F.b2;
+    const std::vector<double>& b3 = F.b3;
     // c[j1,j2,j3] = sign(j1 - max(j2, j3)): group (1,) of mapping_coefficients.
     auto c3 = [&](int j1, int j2, int j3) {
         int b = std::max(j2, j3);
         return j1 > b ? 1.0 : (j1 < b ? -1.0 : 0.0);
     };
     // contract axis 1: t1[j2, j3, k1]
-    std::vector<double> t1((size_t)np * np * h1, 0.0);
+    F.t1.assign((size_t)np * np * h1, 0.0);
     for (int k1 = 0; k1 < h1; ++k1)
         for (int j3 = 0; j3 < np; ++j3)
             for (int j2 = 0; j2 < np; ++j2) {
                 double s = 0;
                 for (int j1 = 0; j1 < np; ++j1) s += c3(j1, j2, j3) * b1[j1 + np * k1];
-                t1[j2 + np * (j3 + (size_t)np * k1)] = s;
-            }
-    // contract axis 2: t2[j3, k1, k2]
-    std::vector<double> t2((size_t)np * h1 * n2, 0.0);
-    for (int k2 = 0; k2 < n2; ++k2)
-        for (int k1 = 0; k1 < h1; ++k1)
-            for (int j3 = 0; j3 < np; ++j3) {
-                double s = 0;
-                for (int j2 = 0; j2 < np; ++j2) s += t1[j2 + np * (j3 + (size_t)np * k1)] * b2[j2 + np * k2];
-                t2[j3 + np * (k1 + (size_t)h1 * k2)] = s;
-            }
-    // contract axis 3: M[k1, k2, k3], then f0
-    m1.assign((size_t)h1 * n2 * n3, 0.0);
-    for (int k3 = 0; k3 < n3; ++k3)
-        for (int k2 = 0; k2 < n2; ++k2)
-            for (int k1 = 0; k1 < h1; ++k1) {
-                double s = 0;
-                const double* tp = &t2[np * (k1 + (size_t)h1 * k2)];
-                for (int j3 = 0; j3 < np; ++j3) s += tp[j3] * b3[j3 + np * k3];
-                m1[k1 + (size_t)h1 * (k2 + (size_t)n2 * k3)] = halfband_split(s, poly);
+                F.t1[j2 + np * (j3 + (size_t)np * k1)] = s;
             }
     // 2-D kernel on (w2, w3): c2[j2, j3] = sign(j2 - j3)
     std::vector<double> t((size_t)np * n3, 0.0);   // t[j2, k3] = sum_j3 c2 b3[j3, k3]
@@ -341,24 +333,48 @@ static void hourglass_tables(const int dims[3], int order, int poly, std::vector
             for (int j3 = 0; j3 < np; ++j3) s += (j2 > j3 ? 1.0 : (j2 < j3 ? -1.0 : 0.0)) * b3[j3 + np * k3];
             t[j2 + np * k3] = s;
         }
-    m2.assign((size_t)n2 * n3, 0.0);
+    F.m2.assign((size_t)n2 * n3, 0.0);
     for (int k3 = 0; k3 < n3; ++k3)
         for (int k2 = 0; k2 < n2; ++k2) {
             double s = 0;
             for (int j2 = 0; j2 < np; ++j2) s += b2[j2 + np * k2] * t[j2 + np * k3];
-            m2[k2 + (size_t)n2 * k3] = halfband_split(s, poly);
+            F.m2[k2 + (size_t)n2 * k3] = halfband_split(s, poly);
         }
+    return F;
+}
+
+// m1 = f0(M1) on the rfft grid: the contraction along axes 2 and 3 (the
+// device design does the same per bin, in the same order).
+void ns_design_fill_m1(NSDesign& D) {
+    if (!D.m1.empty()) return;
+    const NSHourglassFactors& F = D.hg;
+    const int h1 = D.h1, n2 = D.dims[1], n3 = D.dims[2], np = F.np;
+    D.m1.assign((size_t)h1 * n2 * n3, 0.0);
+    std::vector<double> t2(np);
+    for (int k3 = 0; k3 < n3; ++k3)
+        for (int k2 = 0; k2 < n2; ++k2)
+            for (int k1 = 0; k1 < h1; ++k1) {
+                double s = 0;
+                for (int j3 = 0; j3 < np; ++j3) {
+                    double u = 0;
+                    for (int j2 = 0; j2 < np; ++j2) u += F.t1[j2 + np * (j3 + (size_t)np * k1)] * F.b2[j2 + np * k2];
+                    s += u * F.b3[j3 + np * k3];
+                }
+                D.m1[k1 + (size_t)h1 * (k2 + (size_t)n2 * k3)] = halfband_split(s, D.p.halfband_order);
+            }
 }
 
 // src/transforms/ns_surfacelet.jl:98-123, 178-185
-NSDesign ns_design(const sfl_ns_params& p, const int dims[3], bool pyramid) {
+NSDesign ns_design(const sfl_ns_params& p, const int dims[3], bool pyramid, bool with_m1) {
     ns_check_params(p);
     if (pyramid) ns_check_size(p, dims);
     NSDesign D;
     for (int d = 0; d < 3; ++d) D.dims[d] = dims[d];
     D.h1 = dims[0] / 2 + 1;
     D.p = p;
-    hourglass_tables(dims, p.bernstein_order, p.halfband_order, D.m1, D.m2);
+    D.hg = ns_hourglass_factors(dims, p.bernstein_order, p.halfband_order);
+    D.m2 = D.hg.m2;
+    if (with_m1) ns_design_fill_m1(D);
     D.wedges.resize(p.scales);
     for (int j = 0; j < p.scales; ++j) {
         int L = p.direction_levels[j];

@@ -52,11 +52,20 @@ struct WedgePlanes {
     std::vector<std::vector<double>> w;
 };
 
+// The separable parts of the hourglass tables: Bernstein tables of axes 2
+// and 3 ((order + 1) x n), the mapping kernel contracted along axis 1
+// (t1[j2, j3, k1]) and m2.
+struct NSHourglassFactors {
+    int np = 0;
+    std::vector<double> t1, b2, b3, m2;
+};
+
 struct NSDesign {
     int dims[3] = {0, 0, 0};
     int h1 = 0;
     sfl_ns_params p{};
-    std::vector<double> m1;   // f0(M1) on (h1, n2, n3), column-major
+    NSHourglassFactors hg;
+    std::vector<double> m1;   // f0(M1) on (h1, n2, n3), column-major (ns_design_fill_m1; empty until then)
     std::vector<double> m2;   // f0(M2) on (n2, n3)
     // wedges[j][i][plane]: scale j (coarse first), hourglass i, plane a/b;
     // square-rooted when tight.
@@ -78,7 +87,11 @@ void ns_check_size(const sfl_ns_params& p, const int dims[3]);
 int ns_nbands(const sfl_ns_params& p, int j);      // scale j 1-based
 int ns_nsubbands(const sfl_ns_params& p);
 // pyramid = false: the standalone directional bank (no pyramid, no size rule).
-NSDesign ns_design(const sfl_ns_params& p, const int dims[3], bool pyramid = true);
+// with_m1 = false leaves m1 to the device design (ns_design.cu) or to
+// ns_design_fill_m1.
+NSDesign ns_design(const sfl_ns_params& p, const int dims[3], bool pyramid = true, bool with_m1 = true);
+NSHourglassFactors ns_hourglass_factors(const int dims[3], int order, int poly);
+void ns_design_fill_m1(NSDesign& D);
 std::vector<double> ns_hourglass_mask(const NSDesign& D, int i);
 
 // ── Decimated Surfacelet ──────────────────────────────────────────────────────

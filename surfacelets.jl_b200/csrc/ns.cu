@@ -249,25 +249,23 @@ void ns_use_planes(NSPlan& P) {
         throw ArgError("the plane-major pipeline does not support size " + std::to_string(P.dims[0]) + "x" +
                        std::to_string(P.dims[1]) + "x" + std::to_string(P.dims[2]));
     if (!P.Gp.p) {
-        const NSDesign& D = P.design;
-        const int J = P.p.scales;
+        // permute the float32 tables the plan already holds (designed on the device)
         const int h1 = P.h1, n2 = P.dims[1], n3 = P.dims[2];
-        auto permute = [&](const std::vector<double>& g, std::vector<float>& dst) {
-            size_t base = dst.size();
-            dst.resize(base + g.size());
-            for (int k3 = 0; k3 < n3; ++k3)
-                for (int k2 = 0; k2 < n2; ++k2)
-                    for (int k1 = 0; k1 < h1; ++k1)
-                        dst[base + k2 + (size_t)n2 * (k3 + (size_t)n3 * k1)] =
-                            (float)g[k1 + (size_t)h1 * (k2 + (size_t)n2 * k3)];
+        auto permute_all = [&](const DevMem& src, std::vector<float>& dst) {
+            const size_t n = src.p ? src.bytes / sizeof(float) / (size_t)P.H * (size_t)P.H : 0;
+            std::vector<float> g(n);
+            if (n) cuda_check(cudaMemcpy(g.data(), src.p, n * sizeof(float), cudaMemcpyDeviceToHost), "table readback");
+            dst.resize(n);
+            for (size_t base = 0; base < n; base += (size_t)P.H)
+                for (int k3 = 0; k3 < n3; ++k3)
+                    for (int k2 = 0; k2 < n2; ++k2)
+                        for (int k1 = 0; k1 < h1; ++k1)
+                            dst[base + k2 + (size_t)n2 * (k3 + (size_t)n3 * k1)] =
+                                g[base + k1 + (size_t)h1 * (k2 + (size_t)n2 * k3)];
         };
         std::vector<float> Gp, Blp;
-        for (int j = 1; j <= J; ++j)
-            for (int i = 1; i <= 3; ++i)
-                permute(P.ndfb ? ns_hourglass_mask(D, i) : ns_group_mask(D, J - j, i, true), Gp);
-        if (!P.p.tight)
-            for (int lv = 0; lv < J; ++lv)
-                permute(P.ndfb ? std::vector<double>((size_t)P.H, 1.0) : ns_group_mask(D, lv, 1, false), Blp);
+        permute_all(P.G, Gp);
+        if (!P.p.tight) permute_all(P.Bl, Blp);
         upload(P.Gp, Gp);
         upload(P.Blp, Blp);
         P.tbp = P.tb;
@@ -288,7 +286,7 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     for (int d = 0; d < 3; ++d)
         if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
     P.ndfb = ndfb;
-    P.design = ns_design(p, dims, !ndfb);
+    P.design = ns_design(p, dims, !ndfb, false);
     const NSDesign& D = P.design;
     P.p = p;
     for (int d = 0; d < 3; ++d) P.dims[d] = dims[d];
@@ -299,36 +297,10 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     P.nch = dtype == SFL_COMPLEX64 ? 2 : 1;
     const int J = p.scales;
 
-    // tables: group masks (and level bandpasses when not tight), designed in float64
+    // tables: group masks (and level bandpasses when not tight), designed in
+    // float64 on the device, with the support box of each
     NSMaskTables& tb = P.tb;
-    {
-        std::vector<float> G;
-        G.reserve((size_t)3 * J * P.H);
-        P.boxes.clear();
-        for (int j = 1; j <= J; ++j)
-            for (int i = 1; i <= 3; ++i) {
-                std::vector<double> g = ndfb ? ns_hourglass_mask(D, i) : ns_group_mask(D, J - j, i, true);
-                for (double v : g) G.push_back((float)v);
-                P.boxes.push_back(ns_table_box(g, P.h1, dims[1], dims[2]));
-            }
-        upload(P.G, G);
-        std::vector<float> Bl;
-        if (!p.tight) {
-            if (ndfb) {
-                // untight synthesis filters of the standalone bank are all 1
-                Bl.assign((size_t)P.H, 1.0f);
-            } else {
-                for (int lv = 0; lv < J; ++lv) {
-                    std::vector<double> b = ns_group_mask(D, lv, 1, false);
-                    for (double v : b) Bl.push_back((float)v);
-                    // the synthesis bandpass B_j covers the group factors of its level
-                    const NSBox bb = ns_table_box(b, P.h1, dims[1], dims[2]);
-                    for (int i = 0; i < 3; ++i) P.boxes[3 * (J - 1 - lv) + i] = bb;
-                }
-            }
-        }
-        upload(P.Bl, Bl);
-    }
+    ns_design_tables_device(P);
     if (ndfb) {
         P.boxes.push_back(ns_make_box(P.h1, dims[1], dims[1]));   // no lowpass; keeps the table indexing uniform
         P.boxes_full = ns_make_box(P.h1, dims[1], dims[1]);

@@ -164,6 +164,9 @@ void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
 // Plane-major pipeline (ns_plane.cu).
 bool ns_plane_supported(int n1, int n2, int n3);
 void ns_use_planes(NSPlan& P);
+// Group tables G, level bandpasses Bl and the per-table support boxes,
+// designed in float64 on the device (ns_design.cu).
+void ns_design_tables_device(NSPlan& P);
 // Slab pipeline (ns_slab.cu).
 bool ns_slab_supported(int n1, int n2, int n3);
 void ns_use_slabs(NSPlan& P);

@@ -78,6 +78,35 @@ def test_ns_design_tables_match_oracle(sfl, dims, L, order, tr, tight):
             assert np.abs(_ns_table(sfl, t, dims, "pl", lv * 3 + ax) - T.pl[lv][ax]).max() < 1e-15
 
 
+@pytest.mark.parametrize("dims,L,order,tr,tight", [
+    ((16, 12, 20), [1, 2], 6, 1.0, True),
+    ((15, 20, 8), [1, 1, 2], 12, 0.5, False),
+])
+def test_ns_group_tables_match_oracle(sfl, dims, L, order, tr, tight):
+    """The float64 group tables B_j hg_i, the bandpasses B_j and the hourglass
+    masks the plans round to float32 (src/transforms/ns_surfacelet.jl:265-272,
+    src/directional/hourglass.jl:264-289)."""
+    t = sfl.NSSurfacelet(direction_levels=L, bernstein_order=order, transition=tr, tight=tight)
+    p = N.NSParams.make(direction_levels=L, bernstein_order=order, transition=tr, tight=tight)
+    T = N.make_tables(p, dims)
+    h1 = dims[0] // 2 + 1
+    J = len(L)
+    shape = (h1, dims[1], dims[2])
+    for j in range(1, J + 1):
+        for i in (1, 2, 3):
+            got = _ns_table(sfl, t, dims, "group", 3 * (j - 1) + i - 1).reshape(shape, order="F")
+            exp = T.band[J - j] * N.hg_factor(T.m1, T.m2, i, tight)
+            assert np.abs(got - exp).max() < 1e-12
+    for lv in range(J):
+        got = _ns_table(sfl, t, dims, "bandpass", lv).reshape(shape, order="F")
+        assert np.abs(got - T.band[lv]).max() < 1e-12
+    for i in (1, 2, 3):
+        got = _ns_table(sfl, t, dims, "hourglass", i - 1).reshape(shape, order="F")
+        assert np.abs(got - N.hourglass_mask(T.m1, T.m2, i, tight)).max() < 1e-12
+    with pytest.raises(ValueError, match="out of range"):
+        _ns_table(sfl, t, dims, "group", 3 * J)
+
+
 @pytest.mark.parametrize("dims,L,mode,bo", [
     ((48, 48, 48), [[[-1, 1, 1], [1, -1, 1], [1, 1, -1]]] * 2, 1.5, 8),
     ((32, 32, 32), [[[-1, 2, 0], [1, -1, 1], [0, 3, -1]]], 2, 6),
