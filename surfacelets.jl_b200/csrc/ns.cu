@@ -520,13 +520,19 @@ void analyze_items(NSPlan& P, const float2* X, float* cbase, ZMap zc, int es, in
     pass_c2r(P, W, P.H, cbase, zc, es, 1.0f / (float)P.N, nz, st);
 }
 
-// Synthesis accumulation of items [i0, i0 + nz) read from the coefficients
-// (item z at cbase + zc.off(z)) into acc/comp.
-void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz, bool analysis_masks, float2* acc,
-                 float2* comp, bool init, cudaStream_t st) {
-    float2* W = P.work.as<float2>();
+// The forward axis-1 and axis-2 passes of nz subband volumes into work slots
+// slot0.. (one channel).
+void stage_items(NSPlan& P, const float* cbase, ZMap zc, int es, int nz, int slot0, cudaStream_t st) {
+    float2* W = P.work.as<float2>() + (long long)slot0 * P.H;
     pass_r2c(P, cbase, zc, es, W, P.H, nz, st);
     pass_c2c(P, W, W, P.H, 1, false, nz, st);
+}
+
+// The axis-3 pass of work slots 0..nz-1 times the masks of items i0.., summed
+// into acc (Kahan-compensated through comp).
+void accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, bool init,
+                 cudaStream_t st) {
+    float2* W = P.work.as<float2>();
     FFTLen* f3 = get_fft(P.ffts, P.dims[2]);
     int n = f3->sh.n;
     {
@@ -562,6 +568,81 @@ void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz,
                                              f3->sh, T, npad);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "ns_accum_kernel launch");
+}
+
+void synth_items(NSPlan& P, const float* cbase, ZMap zc, int es, int i0, int nz, bool analysis_masks, float2* acc,
+                 float2* comp, bool init, cudaStream_t st) {
+    stage_items(P, cbase, zc, es, nz, 0, st);
+    accum_items(P, i0, nz, analysis_masks, acc, comp, init, st);
+}
+
+// The denoiser's axis-1 step on the line pipeline, one kernel per pair of
+// lines: C2R of the two half-spectrum lines (scaled by 1/N), the soft
+// threshold of subband z's tau on both real lines, and their R2C, in place in
+// the work slots.  The same arithmetic as pass_c2r, soft_threshold_kernel and
+// pass_r2c one after the other, so the result is theirs bit for bit.
+template <int N>
+__global__ void __launch_bounds__(256) reg_shrink_axis1_kernel(RLoadHPair ld, RStoreHalfPair sto,
+                                                               const float2* __restrict__ tw, int nlines,
+                                                               float scale, const float* __restrict__ tau,
+                                                               const NSItem* __restrict__ items, int item0) {
+    using G = RegGeom<N>;
+    constexpr int N1 = G::N1, N2 = G::N2, LP = G::LP;
+    extern __shared__ float2 xch[];
+    const int tid = threadIdx.x;
+    const int p = tid % N2, lp = tid / N2;
+    const int l = blockIdx.x * LP + lp;
+    const int z = blockIdx.y;
+    const bool valid = l < nlines;
+    float2* xl = xch + lp * G::XLINE;
+    const float t = tau[items[item0 + z].s - 1];
+    const RLoadHPair::Ctx lc = ld.line(z, l, valid);
+    float2 u[G::M * N2];
+    reg_line_fft<N, true>(ld, lc, valid, p, xl, tw, u);
+    const bool hasb = lc.b != nullptr;
+#pragma unroll
+    for (int q = 0; q < G::M * N2; ++q) {
+        const float a = __fmul_rn(u[q].x, scale);
+        const float b = hasb ? __fmul_rn(u[q].y, scale) : 0.f;
+        u[q] = make_float2(copysignf(fmaxf(fabsf(a) - t, 0.f), a), hasb ? copysignf(fmaxf(fabsf(b) - t, 0.f), b) : 0.f);
+    }
+    // back to natural order: thread p takes x[p + N2 r]
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < G::M; ++j)
+#pragma unroll
+        for (int k = 0; k < N2; ++k) xl[(p + N2 * j) + N1 * k] = u[j * N2 + k];
+    __syncthreads();
+    float2 v[N1];
+#pragma unroll
+    for (int r = 0; r < N1; ++r) v[r] = xl[p + N2 * r];
+    __syncthreads();
+    reg_line_fft_v<N, false>(v, p, xl, tw, u);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < G::M; ++j)
+#pragma unroll
+        for (int k = 0; k < N2; ++k) xl[(p + N2 * j) + N1 * k] = u[j * N2 + k];
+    __syncthreads();
+    if (valid) sto.staged(sto.line(z, l, valid), xl, p, N2);
+}
+
+template <int N>
+void launch_shrink_axis1(const RLoadHPair& ld, const RStoreHalfPair& sto, const float2* tw, int nlines, int nz,
+                         float scale, const float* tau, const NSItem* items, int item0, cudaStream_t st) {
+    using G = RegGeom<N>;
+    static bool configured = false;
+    if (!configured) {
+        cuda_check(cudaFuncSetAttribute(reg_shrink_axis1_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)G::SMEM),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    dim3 grid((nlines + G::LP - 1) / G::LP, nz);
+    int tok = prof_begin("ns_shrink_axis1", st);
+    reg_shrink_axis1_kernel<N><<<grid, G::THREADS, G::SMEM, st>>>(ld, sto, tw, nlines, scale, tau, items, item0);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "reg_shrink_axis1_kernel launch");
 }
 
 }  // namespace
@@ -600,6 +681,71 @@ void ns_accumulate_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, i
         ns_slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, st);
     else
         synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, comp, false, st);
+}
+
+void ns_stage_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
+                    cudaStream_t st) {
+    if (slot0 < 0 || slot0 + nz > P.group) throw ArgError("work slots out of range");
+    if (P.slab) {
+        ns_slab_stage_items(P, vol, vz, es, i0, nz, slot0, nch, st);
+    } else {
+        if (nch != 1) throw ArgError("the line pipeline stages one channel at a time");
+        stage_items(P, vol, vz, es, nz, slot0, st);
+    }
+}
+
+void ns_accum_staged(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, int nch,
+                     cudaStream_t st) {
+    if (P.slab) {
+        ns_slab_accum_items(P, i0, nz, analysis_masks, acc, nch, st);
+    } else {
+        if (nch != 1) throw ArgError("the line pipeline stages one channel at a time");
+        accum_items(P, i0, nz, analysis_masks, acc, comp, false, st);
+    }
+}
+
+bool ns_line_shrink_supported(const NSPlan& P) {
+    switch (P.dims[0]) {
+        case 16: case 32: case 64: case 96: case 128: case 160: case 256:
+            return true;
+    }
+    return false;
+}
+
+void ns_line_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc, float2* comp,
+                           cudaStream_t st) {
+    float2* W = P.work.as<float2>();
+    Grid hg = half_grid(P);
+    FFTLen* f3 = get_fft(P.ffts, P.dims[2]);
+    Lines g3 = axis_lines(hg.d, 2);
+    ZMap zw;
+    zw.zstride = P.H;
+    if (!launch_reg<true>(f3->sh.n, RLoadNSMask{X, P.tb, P.items.as<NSItem>(), i0, 0}, RStoreC{W, zw, g3},
+                          f3->sh.tw, g3.nlines, nz, true, st, "ns_mask_axis3")) {
+        LoadNSMask ld{X, P.tb, P.items.as<NSItem>(), i0, 0};
+        StoreC sto{W, zw, g3, 1.f};
+        launch_pass(ld, sto, f3->sh, g3.nlines, nz, true, st, "ns_mask_axis3");
+    }
+    pass_c2c(P, W, W, P.H, 1, true, nz, st);
+    FFTLen* f1 = get_fft(P.ffts, P.dims[0]);
+    const Lines gh = axis_lines(hg.d, 0);
+    const int pairs = (axis_lines(P.dims, 0).nlines + 1) / 2;
+    const RLoadHPair ld{W, zw, gh, f1->sh.n};
+    const RStoreHalfPair sto{W, zw, gh, f1->sh.n};
+    const float sc = 1.0f / (float)P.N;
+    const NSItem* it = P.items.as<NSItem>();
+    switch (P.dims[0]) {
+        case 16: launch_shrink_axis1<16>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        case 32: launch_shrink_axis1<32>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        case 64: launch_shrink_axis1<64>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        case 96: launch_shrink_axis1<96>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        case 128: launch_shrink_axis1<128>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        case 160: launch_shrink_axis1<160>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        case 256: launch_shrink_axis1<256>(ld, sto, f1->sh.tw, pairs, nz, sc, tau, it, i0, st); break;
+        default: throw ArgError("no register pass for axis 1 of this size");
+    }
+    pass_c2c(P, W, W, P.H, 1, false, nz, st);
+    accum_items(P, i0, nz, false, acc, comp, false, st);
 }
 
 void ns_inverse_spectrum(NSPlan& P, float2* A, float* x, int es, cudaStream_t st) {
@@ -701,12 +847,25 @@ void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
         ns_plane_stream_synth_push(P, P.stream_pos, band, st);
     } else {
         const long long E = ns_spec_elems(P);
-        for (int ch = 0; ch < P.nch; ++ch) {
-            float2* A = P.acc.as<float2>() + ch * E;
-            float2* K = P.comp.as<float2>() + ch * P.H;
-            if (P.stream_pos == 0) ns_acc_clear(P, A, K, st);
-            ns_accumulate_range(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1, false,
-                                A, K, st);
+        if (P.stream_pos == 0) {
+            for (int ch = 0; ch < P.nch; ++ch) ns_acc_clear(P, P.acc.as<float2>() + ch * E, P.comp.as<float2>() + ch * P.H, st);
+            P.stream_chunk0 = 0;
+        }
+        if (P.slab || P.nch == 1) {
+            // stage the subband in the work slot of its position in the mask
+            // group; the axis-3 accumulation runs once per group
+            const int c0 = P.stream_chunk0, c1 = ns_next_chunk(P, c0);
+            ns_stage_range(P, reinterpret_cast<const float*>(band), ZMap{}, P.nch, P.stream_pos, 1,
+                           P.stream_pos - c0, P.nch, st);
+            if (P.stream_pos + 1 == c1) {
+                ns_accum_staged(P, c0, c1 - c0, false, P.acc.as<float2>(), P.comp.as<float2>(), P.nch, st);
+                P.stream_chunk0 = c1;
+            }
+        } else {
+            // complex data on the line pipeline: the work slots hold one channel
+            for (int ch = 0; ch < P.nch; ++ch)
+                ns_accumulate_range(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1,
+                                    false, P.acc.as<float2>() + ch * E, P.comp.as<float2>() + ch * P.H, st);
         }
     }
     P.stream_pos += 1;

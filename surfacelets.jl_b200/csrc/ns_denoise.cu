@@ -3,7 +3,9 @@
 // pipeline every subband stays on the chip: the analysis axis-3 pass, one
 // slab pass that inverts, thresholds and re-transforms (ns_slab_shrink_kernel)
 // and the synthesis accumulation, so the coefficients never reach HBM.  The
-// line pipeline goes through a float32 scratch of one chunk of subbands.
+// line pipeline fuses its axis-1 C2R, the threshold and the axis-1 R2C into
+// one kernel on the work slots (axis-1 lengths with a register kernel), or
+// else goes through a float32 scratch of one chunk of subbands.
 // Either way the result equals synthesize(soft(analyze(x))) of the same
 // pipeline bit for bit.
 #include "plan.h"
@@ -33,7 +35,8 @@ void ns_denoise(NSPlan& P, const float* x, float* y, const float* tau, cudaStrea
     float2* K = P.comp.as<float2>();
     ns_forward_spectrum(P, x, 1, X, st);
     ns_acc_clear(P, A, K, st);
-    if (!P.slab) {
+    const bool fused_lines = !P.slab && ns_line_shrink_supported(P);
+    if (!P.slab && !fused_lines) {
         const size_t need = sizeof(float) * (size_t)P.N * P.group;
         if (P.band.bytes < need) P.band.alloc(need);
     }
@@ -44,6 +47,10 @@ void ns_denoise(NSPlan& P, const float* x, float* y, const float* tau, cudaStrea
         const int nz = i1 - i0;
         if (P.slab) {
             ns_slab_denoise_items(P, X, i0, nz, tau, A, st);
+            continue;
+        }
+        if (fused_lines) {
+            ns_line_denoise_items(P, X, i0, nz, tau, A, K, st);
             continue;
         }
         float* band = P.band.as<float>();

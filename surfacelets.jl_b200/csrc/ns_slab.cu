@@ -39,14 +39,11 @@
 #include "plan.h"
 #include "prof.h"
 #include "regpass.cuh"
+#include "slab_core.cuh"
 
 namespace sfl {
 
 namespace {
-
-constexpr int kSlabThreads = 512;
-constexpr int kSlabWarps = kSlabThreads / 32;
-constexpr size_t kSlabSmemMax = 112 * 1024;   // two CTAs an SM
 
 // ── lines along axis 3 of a padded spectrum, restricted to a box ───────────
 
@@ -247,100 +244,6 @@ __global__ void __launch_bounds__(256, 2) ns_slab_accum_kernel(const float2* __r
 }
 
 // ── slab passes ─────────────────────────────────────────────────────────────
-
-struct SlabArgs {
-    float2* spec;            // padded spectra, item z at spec + z * spec_zstride
-    long long spec_zstride;
-    float* vol;              // real volumes (element stride es), item z at vol + vz.off(z)
-    ZMap vz;
-    int es;
-    float scale;             // applied to the C2R outputs
-    int P1, n3;
-    int nk1, nk2, b2;        // box: rows k1 < nk1, columns as BoxMap
-    int units;               // channels x items x n3
-    int nzc;                 // items a channel
-    long long spec_chstride; // spectra: channel stride (the volume's channels are interleaved floats)
-    const float2* twa;       // w_n1^k, k < n1 (float64-designed)
-    const float2* twb;       // w_n2^k, k < n2
-    const float* tau;        // shrink pass: threshold of subband s at tau[s - 1]
-    const NSItem* items;     // shrink pass: the launch's items, from item0
-    int item0;
-};
-
-template <int N>
-struct SlabLine {
-    static constexpr int N1 = LinePlan<N>::N1;
-    static constexpr int N2 = LinePlan<N>::N2;
-    static constexpr int M = N1 / N2;
-    static constexpr int LPW = 32 / N2;             // lines a warp
-    static constexpr int LPR = kSlabWarps * LPW;    // lines a round
-};
-
-// Twiddles of a line FFT rearranged as tw2[m * N2 + p] = w_N^{p m}: the N2
-// lanes of a line read consecutive words.
-template <int N>
-__device__ __forceinline__ void load_slab_twiddles(float2* tw2, const float2* __restrict__ tw) {
-    using L = SlabLine<N>;
-    for (int i = threadIdx.x; i < L::N1 * L::N2; i += blockDim.x) {
-        const int m = i / L::N2, p = i - m * L::N2;
-        tw2[i] = tw[p * m];
-    }
-}
-
-// Axis-1 pitch of a padded spectrum with h1 bins on axis 1: the smallest
-// P1 >= h1 with P1 = 2 mod 4.
-constexpr int slab_pitch_c(int h1) { return h1 % 4 == 2 ? h1 : slab_pitch_c(h1 + 1); }
-
-// FFT of one line of N points held by the N2 lanes p of a warp: v[r] holds
-// x[p + N2 r] on entry and X[(p + N2 j) + N1 k] at v[j N2 + k] on exit.  The
-// exchange runs through the line's own slots base[STRIDE t], t < N, with
-// slot (sender q, value m) at t = N2 m + (q ^ (m mod N2)): conflict-free
-// writes and reads for STRIDE = 1 and for STRIDE = 2 mod 4.  Lanes of
-// invalid lines skip every slot access but keep to the warp barriers.
-template <int N, bool INV, int STRIDE>
-__device__ __forceinline__ void warp_line_fft(float2 (&v)[LinePlan<N>::N1], int p, bool valid,
-                                              const float2* __restrict__ tw2, float2* base) {
-    using L = SlabLine<N>;
-    constexpr int N1 = L::N1, N2 = L::N2;
-    RegDft<N1, INV>::run(v);
-#pragma unroll
-    for (int m = 1; m < N1; ++m) {
-        float2 w = tw2[m * N2 + p];
-        if (INV) w.y = -w.y;
-        v[m] = c_mul(v[m], w);
-    }
-    // x[c] = STRIDE (p ^ c): the sender-dependent part of a slot, shared by both sides
-    int xo[N2];
-#pragma unroll
-    for (int c = 0; c < N2; ++c) xo[c] = STRIDE * (p ^ c);
-    __syncwarp();   // the line's inputs may have come from its own slots
-    if (valid) {
-#pragma unroll
-        for (int m = 0; m < N1; ++m) base[xo[m & (N2 - 1)] + STRIDE * N2 * m] = v[m];
-    }
-    __syncwarp();
-    const float2* rb = base + STRIDE * N2 * p;
-#pragma unroll
-    for (int j = 0; j < L::M; ++j) {
-        float2 w[N2];
-#pragma unroll
-        for (int pp = 0; pp < N2; ++pp)
-            w[pp] = valid ? rb[xo[pp] + STRIDE * N2 * N2 * j] : make_float2(0.f, 0.f);
-        RegDft<N2, INV>::run(w);
-#pragma unroll
-        for (int k = 0; k < N2; ++k) v[j * N2 + k] = w[k];
-    }
-    __syncwarp();   // slots are free again
-}
-
-// Lane layout of the column-pair phases: p fastest, then the line; with four
-// lines a warp, the two lines of a half warp are two apart so that their
-// columns fall on disjoint banks (P1 = 2 mod 4).
-template <int N>
-__device__ __forceinline__ int pair_subline(int s) {
-    if (SlabLine<N>::LPW == 4) return s == 1 ? 2 : (s == 2 ? 1 : s);
-    return s;
-}
 
 // Analysis slab pass (inverse): spectra -> real volumes (element stride ES).
 // The exchange slots of a column pair are the pair's two columns read as one
@@ -769,6 +672,10 @@ bool launch_slab_n(int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t
 
 template <int KIND>
 void launch_slab(int na, int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
+    if (slab_cluster_supported(na, nb)) {
+        if (!launch_slab_cluster(KIND, na, nb, a, sms, st, tag)) throw ArgError("no slab kernel for this size");
+        return;
+    }
     bool ok = false;
     switch (na) {
         case 64: ok = launch_slab_n<KIND, 64>(nb, a, sms, smem, st, tag); break;
@@ -980,21 +887,28 @@ void slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es,
     launch_slab<1>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_c2r");
 }
 
-// Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
-// vol + vz.off(z) (+ ch) into acc + ch SP.
-void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
-                      float2* acc, int nch, cudaStream_t st) {
+// Synthesis staging of items [i0, i0 + nz) (one mask group) read from
+// vol + vz.off(z) (+ ch): slab R2C into work slots slot0.. (+ ch group SP).
+void slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
+                      cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     prof_bytes("ns_slab_r2c", nch * nz * (4.0 * P.N + box_bytes(P, b)));
     SlabArgs a = slab_args(P, b, nz);
     a.units *= nch;
     a.spec_chstride = ych_stride(P);
-    a.spec = P.work.as<float2>();
+    a.spec = P.work.as<float2>() + (long long)slot0 * P.SP;
     a.spec_zstride = P.SP;
     a.vol = const_cast<float*>(vol);
     a.vz = vz;
     a.es = es;
     launch_slab<0>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_r2c");
+}
+
+// Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
+// vol + vz.off(z) (+ ch) into acc + ch SP.
+void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
+                      float2* acc, int nch, cudaStream_t st) {
+    slab_stage_items(P, vol, vz, es, i0, nz, 0, nch, st);
     slab_accum_pass(P, i0, nz, analysis_masks, acc, nch, st);
 }
 
@@ -1028,7 +942,8 @@ int chunk_end(const NSPlan& P, int i0) {
 }  // namespace
 
 bool ns_slab_supported(int n1, int n2, int n3) {
-    return slab_len(n1) && slab_len(n2) && reg_fft_supported(n3) && slab_smem(n1, n2) <= kSlabSmemMax;
+    if (!reg_fft_supported(n3)) return false;
+    return (slab_len(n1) && slab_len(n2) && slab_smem(n1, n2) <= kSlabSmemMax) || slab_cluster_supported(n1, n2);
 }
 
 // Support box of a table on the rfft grid (h1, n2, n3), k1 fastest.
@@ -1112,6 +1027,15 @@ void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, i
 void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
                            cudaStream_t st) {
     slab_denoise_items(P, X, i0, nz, tau, acc, st);
+}
+
+void ns_slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
+                         cudaStream_t st) {
+    slab_stage_items(P, vol, vz, es, i0, nz, slot0, nch, st);
+}
+
+void ns_slab_accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, int nch, cudaStream_t st) {
+    slab_accum_pass(P, i0, nz, analysis_masks, acc, nch, st);
 }
 
 }  // namespace sfl

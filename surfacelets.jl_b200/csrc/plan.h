@@ -131,6 +131,7 @@ struct NSPlan {
     // streaming state
     int stream_mode = 0;    // 0 idle, 1 analyzing, 2 synthesizing
     int stream_pos = 0;
+    int stream_chunk0 = 0;  // synthesis: first item of the mask group being staged
     NSDesign design;        // kept for the table export
 };
 
@@ -184,6 +185,16 @@ void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, i
                          float2* acc, cudaStream_t st);
 void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
                            cudaStream_t st);
+void ns_slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
+                         cudaStream_t st);
+void ns_slab_accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, int nch, cudaStream_t st);
+// The line pipeline's denoiser step on items [i0, i0 + nz): the analysis
+// axis-3 and axis-2 passes, one fused axis-1 kernel (C2R, soft threshold,
+// R2C), the synthesis axis-2 pass and the accumulation (ns.cu); for axis-1
+// lengths with a register kernel.
+bool ns_line_shrink_supported(const NSPlan& P);
+void ns_line_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc, float2* comp,
+                           cudaStream_t st);
 // Fused soft-threshold denoiser y = S(soft(A x, tau)) (ns_denoise.cu).
 void ns_denoise(NSPlan& P, const float* x, float* y, const float* tau, cudaStream_t st);
 // Item-range building blocks of the slab and line pipelines (ns.cu): the
@@ -199,6 +210,13 @@ void ns_acc_clear(NSPlan& P, float2* acc, float2* comp, cudaStream_t st);
 void ns_accumulate_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
                          float2* acc, float2* comp, cudaStream_t st);
 void ns_inverse_spectrum(NSPlan& P, float2* A, float* x, int es, cudaStream_t st);
+// ns_accumulate_range in two halves: the forward transforms of nz volumes into
+// work slots slot0.. (nch channels on the slab pipeline, 1 on the line
+// pipeline), then the accumulation of items [i0, i0 + nz) from slots 0..nz-1.
+void ns_stage_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
+                    cudaStream_t st);
+void ns_accum_staged(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, int nch,
+                     cudaStream_t st);
 ZMap ns_subband_map(const NSPlan& P, int i0, int es);
 // bfloat16 coefficients with a float32 scale per subband (ns_bf16.cu).
 void ns_analyze_bf16(NSPlan& P, const float* x, void* c, float* scales, cudaStream_t st);

@@ -22,6 +22,10 @@ def soft(c, tau):
     ((64, 64, 64), "lines", dict(scales=3, direction_levels=[2, 2, 3])),
     ((128, 96, 64), "slabs", dict(scales=2, direction_levels=[2, 3], bernstein_order=8)),
     ((40, 36, 48), "lines", dict(scales=2, direction_levels=[1, 2], bernstein_order=6, tight=False)),
+    # fused axis-1 kernel on the line pipeline, an odd number of axis-1 lines (the last pair is one line)
+    ((64, 33, 35), "lines", dict(scales=2, direction_levels=[2, 1], bernstein_order=6)),
+    ((256, 32, 33), "lines", dict(scales=1, direction_levels=[2], bernstein_order=6, tight=False)),
+    ((96, 40, 24), "lines", dict(scales=2, direction_levels=[1, 1], bernstein_order=6)),
 ])
 def test_denoise_equals_three_calls(sfl, dims, pipeline, kw):
     ws = sfl.make_workspace(sfl.NSSurfacelet(**kw), "float32", dims)

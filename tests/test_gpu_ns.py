@@ -167,6 +167,27 @@ def test_streaming_equals_materialized_bit_for_bit(sfl, dims, pipeline, dtype):
     assert rel_l2(sfl.to_host(y), x) <= REL
 
 
+@pytest.mark.parametrize("pipeline,dims", [("lines", (20, 16, 12)), ("slabs", (64, 64, 32))])
+def test_streaming_synthesis_stages_mask_groups(sfl, pipeline, dims):
+    """Streaming synthesis stages each pushed subband and accumulates once per
+    mask group; equal bit for bit to synthesize at group sizes 1, 3 and 8."""
+    import torch
+    t = sfl.NSSurfacelet(scales=2, direction_levels=[2, 3], bernstein_order=6)
+    x = sfl.to_device(np.random.default_rng(6).standard_normal(dims).astype(np.float32))
+    for g in (1, 3, 8):
+        ws = sfl.make_workspace(t, "float32", dims, group=g)
+        ws.set_pipeline(pipeline)
+        c = sfl.analyze(ws, x)
+        y = sfl.volume_like(dims)
+        sfl.synthesize_(lambda i: c[..., i - 1], y, ws)
+        assert torch.equal(y, sfl.synthesize(ws, c)), g
+        wa = sfl.make_workspace(t, "float32", dims, group=g)
+        wa.set_pipeline(pipeline)
+        y2 = sfl.volume_like(dims)
+        sfl.analyze_synthesize_stream(lambda i, b: b, y2, x, wa, ws)
+        assert torch.equal(y2, y), g
+
+
 def test_group_size_does_not_change_results(sfl):
     dims = (20, 16, 12)
     t = sfl.NSSurfacelet(scales=2, direction_levels=[2, 3], bernstein_order=6)
