@@ -117,11 +117,19 @@ struct L3LoadMask {
     }
 };
 
+// Resident CTAs an SM the register budget aims at: two (128 registers a
+// thread) where the line geometry fits, one for the long-N1 lengths 96 and
+// 160 (24 and 40 values a thread) and for 256 in the accumulation.
+template <int N>
+constexpr int mask_minb() { return (N == 96 || N == 160) ? 1 : 2; }
+template <int N>
+constexpr int accum_minb() { return (N == 96 || N == 160 || N >= 256) ? 1 : 2; }
+
 // Analysis line pass over IPC subbands of one mask group per CTA: a line's X
 // times the group factor is loaded once, then per subband scaled by its two
 // wedge planes, transformed along axis 3 and stored.
 template <int N, int IPC>
-__global__ void __launch_bounds__(256) ns_slab_mask_group_kernel(const float2* __restrict__ X, int P1, int s3,
+__global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel(const float2* __restrict__ X, int P1, int s3,
                                                                  BoxMap bx, NSMaskTables tb,
                                                                  const NSItem* __restrict__ items, int item0, int nz,
                                                                  int synth, float2* Y, long long ystride,
@@ -180,7 +188,7 @@ __global__ void __launch_bounds__(256) ns_slab_mask_group_kernel(const float2* _
 // Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
 // summed in registers into the accumulator (plain float32 sums, item order).
 template <int N>
-__global__ void __launch_bounds__(256, 2) ns_slab_accum_kernel(const float2* __restrict__ Y, long long ystride, int G,
+__global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(const float2* __restrict__ Y, long long ystride, int G,
                                                             int P1, int s3, BoxMap bx, NSMaskTables tb,
                                                             const NSItem* __restrict__ items, int item0, int synth,
                                                             float2* acc, const float2* __restrict__ tw, int nlines,
