@@ -167,6 +167,7 @@ def kernel_bytes(tag, P, launches_per_step, nz_total):
 
 
 def main():
+    global DIMS, NS_KW
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -176,11 +177,19 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/secondary/cpu legs")
     ap.add_argument("--group", type=int, default=0, help="subbands in flight per launch (0: the plan's default)")
     ap.add_argument("--workspaces", type=int, default=4, help="graph mode: workspaces (concurrent branches, <= 8)")
+    ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
+                    help="volume size (a smaller or larger case for profiling; the extra lines need the default)")
+    ap.add_argument("--levels", type=int, nargs="+", default=NS_KW["direction_levels"],
+                    help="direction levels per scale (scales = their count)")
     ap.add_argument("--mode", default="graph", choices=["graph", "calls"],
                     help="graph: the batch as one CUDA graph over up to 4 workspaces (sfl_batch_*); "
                          "calls: a loop of plain calls on one workspace")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if tuple(args.dims) != DIMS or list(args.levels) != NS_KW["direction_levels"]:
+        DIMS = tuple(args.dims)
+        NS_KW = dict(scales=len(args.levels), direction_levels=list(args.levels))
+        args.no_extras = True   # the extra lines are defined on the default workload
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -301,17 +310,19 @@ def main():
     achieved = alg / (dom_ms / 1e3) / 1e9 if alg else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
+    if os.path.exists(tfile) and DIMS == (128, 128, 128) and S == 49:   # the captured workload
         tj = json.load(open(tfile)).get(dom)
         if tj:
             traffic = tj.get("bytes_per_launch_full_size")
-    op_bytes = 600.0 * N * B * world     # 4(1+S)*3 B a voxel at S = 49
+    op_bytes = 12.0 * (1 + S) * N * B * world     # 4(1+S)*3 B a voxel: 600 at S = 49
     line = {
         "metric": METRIC, "value": value, "unit": "Mvoxels/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "NSSurfacelet(scales=3, direction_levels=[2,2,3]) 128^3 float32, "
-                               "analyze+synthesize+adjoint(synthesize) per volume",
+        "config": {"workload": f"NSSurfacelet(scales={NS_KW['scales']}, direction_levels="
+                               f"[{','.join(str(v) for v in NS_KW['direction_levels'])}]) "
+                               + ("128^3" if DIMS == (128, 128, 128) else "x".join(str(d) for d in DIMS))
+                               + " float32, analyze+synthesize+adjoint(synthesize) per volume",
                    "batch_per_gpu": B, "global_batch": B * world, "volume": list(DIMS),
                    "parallelism": f"replicas x{world} (no collective)",
                    "execution": ("one CUDA graph a step (sfl_batch_*): volume b on workspace b mod "
@@ -326,7 +337,7 @@ def main():
                      "peak_kind": peak_kind,
                      "launches_per_step": dom_launches, "ms_per_step": dom_ms,
                      "share_of_kernel_time": dom_ms / sum(v[0] for v in per_tag.values())},
-        "op_roofline": {"algorithmic_bytes_per_voxel": 600, "achieved_gbs": op_bytes / (ms / 1e3) / 1e9 / world,
+        "op_roofline": {"algorithmic_bytes_per_voxel": 12 * (1 + S), "achieved_gbs": op_bytes / (ms / 1e3) / 1e9 / world,
                         "frac": op_bytes / (ms / 1e3) / 1e9 / world / hbm, "peak_kind": peak_kind},
         "kernel_ms_per_step": {k: v[0] for k, v in per_tag.items()},
         "kernel_algorithmic_gbs": {k: tag_bytes[k] / (v[0] / 1e3) / 1e9 for k, v in per_tag.items()
