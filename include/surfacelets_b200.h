@@ -300,7 +300,8 @@ int sfl_ns_denoise(sfl_plan* plan, const void* x, void* y, const float* tau, voi
  *   inverse_spectrum   x from an accumulated spectrum (A is overwritten).
  * Accumulated spectra add: the sum over devices of each device's
  * accumulation of its own ranges is the accumulation of all of them.  Slab
- * and line pipelines only; not while a stream is open. */
+ * and line pipelines only; not while a stream is open.  X and A are
+ * 16-byte aligned device buffers. */
 int sfl_ns_spectrum_elems(const sfl_plan* plan, int64_t* elems);
 int sfl_ns_stream_order(const sfl_plan* plan, int32_t* subband_index);
 int sfl_ns_forward_spectrum(sfl_plan* plan, const void* x, void* X, void* stream);

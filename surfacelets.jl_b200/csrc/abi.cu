@@ -98,6 +98,11 @@ void check_aligned(const void* p, int dtype, const char* what) {
         throw sfl::ArgError(std::string(what) + " is not aligned to its element type");
 }
 
+// Spectra (the item-range ABI) are copied in 16-byte blocks by the slab passes.
+void check_spectrum_aligned(const void* p, const char* what) {
+    if (reinterpret_cast<uintptr_t>(p) % 16 != 0) throw sfl::ArgError(std::string(what) + " is not 16-byte aligned");
+}
+
 // Runs f with the plan's device current, restoring the caller's afterwards.
 template <class F>
 void on_device(const sfl_plan* plan, F&& f) {
@@ -938,6 +943,7 @@ int sfl_ns_forward_spectrum(sfl_plan* plan, const void* x, void* X, void* stream
         sfl::NSPlan& N = range_plan(plan);
         need(x, "x");
         need(X, "X");
+        check_spectrum_aligned(X, "X");
         check_aligned(x, plan->impl.dtype, "x");
         const long long E = sfl::ns_spec_elems(N);
         on_device(plan, [&] {
@@ -953,6 +959,7 @@ int sfl_ns_analyze_range(sfl_plan* plan, const void* X, int32_t first, int32_t c
     return guarded([&] {
         sfl::NSPlan& N = range_plan(plan);
         need(X, "X");
+        check_spectrum_aligned(X, "X");
         need(c, "c");
         check_aligned(c, plan->impl.dtype, "c");
         check_range(N, first, count);
@@ -978,6 +985,7 @@ int sfl_ns_accumulate_range(sfl_plan* plan, const void* c, int32_t first, int32_
         sfl::NSPlan& N = range_plan(plan);
         need(c, "c");
         need(A, "A");
+        check_spectrum_aligned(A, "A");
         check_aligned(c, plan->impl.dtype, "c");
         check_range(N, first, count);
         const long long E = sfl::ns_spec_elems(N);
@@ -1003,6 +1011,7 @@ int sfl_ns_inverse_spectrum(sfl_plan* plan, void* A, void* x, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = range_plan(plan);
         need(A, "A");
+        check_spectrum_aligned(A, "A");
         need(x, "x");
         check_aligned(x, plan->impl.dtype, "x");
         const long long E = sfl::ns_spec_elems(N);

@@ -33,6 +33,7 @@
 // swizzle, so it needs only __syncwarp; CTA-wide barriers separate the
 // phases.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "ns_mask.cuh"
@@ -40,6 +41,7 @@
 #include "prof.h"
 #include "regpass.cuh"
 #include "slab_core.cuh"
+#include "tma.cuh"
 
 namespace sfl {
 
@@ -253,6 +255,60 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
 
 // ── slab passes ─────────────────────────────────────────────────────────────
 
+// ── box rows between HBM and shared memory by bulk copies ──────────────────
+//
+// One cp.async.bulk a box column: the rows k1 < nk1 rounded up to an even
+// count (16-byte multiples; the slab pitch P1 = 2 mod 4 is even, so every
+// column starts 16-byte aligned).  The extra bin of an odd nk1 lies outside
+// the box and is read by no one.  Loads complete on an mbarrier whose wait
+// is bounded; stores are waited on for their shared-memory reads only.
+
+// The slab pass's mbarrier, after the slab in shared memory.
+template <int NA, int NB>
+__device__ __forceinline__ uint64_t* slab_bar(float2* sm) {
+    constexpr int P1 = slab_pitch_c(NA / 2 + 1);
+    return reinterpret_cast<uint64_t*>(sm + NA + NB + P1 * NB);
+}
+
+__device__ __forceinline__ void slab_bar_init(uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+}
+
+template <int NB, int P1>
+__device__ __forceinline__ void slab_bulk_load(float2* S, const float2* src, int nk1, int nk2, int b2,
+                                               uint64_t* bar, uint32_t& phase, int* status) {
+    const uint32_t bytes = (uint32_t)(((nk1 + 1) & ~1) * sizeof(float2));
+    fence_proxy_async();   // this thread's earlier accesses to S ahead of the copies' writes
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, bytes * (uint32_t)nk2);
+    __syncthreads();
+    if ((int)threadIdx.x < nk2) {
+        const int j = threadIdx.x;
+        const int k2 = j <= b2 ? j : j + (NB - nk2);
+        bulk_load(S + P1 * k2, src + P1 * k2, bytes, bar);
+    }
+    mbar_wait_bounded(bar, phase, status);
+    phase ^= 1;
+}
+
+template <int NB, int P1>
+__device__ __forceinline__ void slab_bulk_store(float2* dst, const float2* S, int nk1, int nk2, int b2) {
+    const uint32_t bytes = (uint32_t)(((nk1 + 1) & ~1) * sizeof(float2));
+    fence_proxy_async();   // this thread's writes of S visible to the copies
+    __syncthreads();
+    if ((int)threadIdx.x < nk2) {
+        const int j = threadIdx.x;
+        const int k2 = j <= b2 ? j : j + (NB - nk2);
+        bulk_store(dst + P1 * k2, S + P1 * k2, bytes);
+        bulk_commit();
+        bulk_wait_read();   // S is rewritten by the next unit
+    }
+    __syncthreads();
+}
+
 // Analysis slab pass (inverse): spectra -> real volumes (element stride ES).
 // The exchange slots of a column pair are the pair's two columns read as one
 // run of 2 P1 >= NA values.
@@ -272,17 +328,16 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
     const int k2hi = NB - (nk2 - b2 - 1);   // first negative-frequency column in the box
+    uint64_t* bar = slab_bar<NA, NB>(sm);
+    uint32_t phase = 0;
+    slab_bar_init(bar);
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
         const int per = a.nzc * a.n3;
         const int ch = u / per, ur = u - ch * per;
         const int z = ur / a.n3, s3 = ur - z * a.n3;
         const float2* src = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         // 1. the box of the slab into shared memory
-        for (int j = warp; j < nk2; j += kSlabWarps) {
-            const int k2 = j <= b2 ? j : j + (NB - nk2);
-            for (int k1 = lane; k1 < nk1; k1 += 32) S[k1 + P1 * k2] = src[k1 + P1 * k2];
-        }
-        __syncthreads();
+        slab_bulk_load<NB, P1>(S, src, nk1, nk2, b2, bar, phase, a.status);
         // 2. inverse FFT along axis 2 of the rows k1 < nk1; columns outside the box are zero
         {
             const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
@@ -456,11 +511,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
         __syncthreads();
         // 3. the box of the slab out to the spectrum
         float2* dst = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
-        for (int j = warp; j < nk2; j += kSlabWarps) {
-            const int k2 = j <= b2 ? j : j + (NB - nk2);
-            for (int k1 = lane; k1 < nk1; k1 += 32) dst[k1 + P1 * k2] = S[k1 + P1 * k2];
-        }
-        __syncthreads();   // the slab buffer is reused by the next unit
+        slab_bulk_store<NB, P1>(dst, S, nk1, nk2, b2);   // ends with the barrier before S is reused
     }
 }
 
@@ -488,17 +539,16 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_shrink_kernel(Slab
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
     const int k2hi = NB - (nk2 - b2 - 1);
+    uint64_t* bar = slab_bar<NA, NB>(sm);
+    uint32_t phase = 0;
+    slab_bar_init(bar);
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
         const int per = a.nzc * a.n3;
         const int ch = u / per, ur = u - ch * per;
         const int z = ur / a.n3, s3 = ur - z * a.n3;
         float2* slab = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         const float tau = a.tau[a.items[a.item0 + z].s - 1];
-        for (int j = warp; j < nk2; j += kSlabWarps) {
-            const int k2 = j <= b2 ? j : j + (NB - nk2);
-            for (int k1 = lane; k1 < nk1; k1 += 32) S[k1 + P1 * k2] = slab[k1 + P1 * k2];
-        }
-        __syncthreads();
+        slab_bulk_load<NB, P1>(S, slab, nk1, nk2, b2, bar, phase, a.status);
         {   // inverse FFT along axis 2 of the box rows
             const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
             for (int base = 0; base < nk1; base += LB::LPR) {
@@ -619,11 +669,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_shrink_kernel(Slab
             }
         }
         __syncthreads();
-        for (int j = warp; j < nk2; j += kSlabWarps) {
-            const int k2 = j <= b2 ? j : j + (NB - nk2);
-            for (int k1 = lane; k1 < nk1; k1 += 32) slab[k1 + P1 * k2] = S[k1 + P1 * k2];
-        }
-        __syncthreads();   // the slab buffer is reused by the next unit
+        slab_bulk_store<NB, P1>(slab, S, nk1, nk2, b2);   // ends with the barrier before S is reused
     }
 }
 
@@ -698,7 +744,9 @@ bool slab_len(int n) { return n == 64 || n == 96 || n == 128 || n == 160; }
 
 int slab_pitch(int h1) { return slab_pitch_c(h1); }
 
-size_t slab_smem(int n1, int n2) { return sizeof(float2) * ((size_t)n1 + n2 + (size_t)slab_pitch(n1 / 2 + 1) * n2); }
+size_t slab_smem(int n1, int n2) {
+    return sizeof(float2) * ((size_t)n1 + n2 + (size_t)slab_pitch(n1 / 2 + 1) * n2) + 16;   // + the mbarrier
+}
 
 // ── drivers ──────────────────────────────────────────────────────────────────
 
@@ -723,6 +771,7 @@ SlabArgs slab_args(const NSPlan& P, const NSBox& b, int nz) {
     a.twb = P.ffts.at(P.dims[1])->sh.tw;
     a.es = 1;
     a.scale = 1.f;
+    a.status = P.status.as<int>();
     return a;
 }
 
@@ -775,7 +824,17 @@ void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, 
 
 // Subbands a CTA of the analysis line pass takes: the line's X and group
 // factor are loaded once for all of them.
-int mask_ipc(int nz) { return nz >= 4 ? 4 : (nz >= 2 ? 2 : 1); }
+// Subbands a CTA of the analysis axis-3 pass: up to 4, or at most
+// SFL_MASK_IPC (1, 2 or 4) from the environment, read once.
+int mask_ipc(int nz) {
+    static const int cap = [] {
+        const char* e = std::getenv("SFL_MASK_IPC");
+        const int v = e ? std::atoi(e) : 4;
+        return v >= 4 ? 4 : (v >= 2 ? 2 : 1);
+    }();
+    const int m = std::min(nz, cap);
+    return m >= 4 ? 4 : (m >= 2 ? 2 : 1);
+}
 
 template <int N>
 void launch_mask_group(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,

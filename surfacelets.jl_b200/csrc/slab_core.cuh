@@ -30,6 +30,7 @@ struct SlabArgs {
     const float* tau;        // shrink pass: threshold of subband s at tau[s - 1]
     const NSItem* items;     // shrink pass: the launch's items, from item0
     int item0;
+    int* status;             // the plan's device status word (bounded waits record a timeout there)
 };
 
 template <int N>
