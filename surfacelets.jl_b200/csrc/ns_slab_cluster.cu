@@ -2,9 +2,10 @@
 // up: 130 x 256 complex bins are 266 KB), split over the two CTAs of a
 // thread-block cluster through distributed shared memory.
 //
-// CTA rank r of a cluster holds the rows k1 in [r R, r R + R), R = ceil(h1/2),
-// of the slab's box, at S[(k1 - r R) + PL k2] in its own shared memory
-// (PL = 2 mod 4, >= R).  The axis-2 phase (a row's FFT) is local: each CTA
+// CTA rank 0 of a cluster holds the rows k1 < R of the slab's box, rank 1
+// the rows k1 >= R (R = NA/4, even, so that both blocks of a column start on
+// a 16-byte boundary and move by one cp.async.bulk each), at
+// S[(k1 - r R) + PL k2] in its own shared memory (PL = 2 mod 4).  The axis-2 phase (a row's FFT) is local: each CTA
 // transforms its own rows.  The axis-1 phase (the C2R / R2C of a column pair)
 // needs all h1 rows of two columns: CTA r takes the column pairs
 // [r NB/4, (r + 1) NB/4) and reads (or writes) the rows of the other half in
@@ -27,6 +28,7 @@
 
 #include "prof.h"
 #include "slab_core.cuh"
+#include "tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -39,36 +41,57 @@ constexpr int kClusterCTAs = 2;
 template <int NA, int NB>
 struct ClusterSlab {
     static constexpr int H1 = NA / 2 + 1;
-    static constexpr int R = (H1 + kClusterCTAs - 1) / kClusterCTAs;   // rows a CTA
-    static constexpr int PL = slab_pitch_c(R);
+    static constexpr int R = NA / 4;                                // rows of rank 0; rank 1 has H1 - R
+    static constexpr int PL = slab_pitch_c(H1 - R);
     static constexpr int P1 = slab_pitch_c(H1);                     // pitch of the spectra in HBM
     static constexpr int PAIRS = NB / 2 / kClusterCTAs;             // column pairs a CTA
     static constexpr int LINES = kSlabWarps * SlabLine<NA>::LPW;    // axis-1 lines in flight a CTA
-    // twiddles (NA + NB), the rows (PL NB), the axis-1 exchange (LINES NA)
-    static constexpr size_t SMEM = sizeof(float2) * ((size_t)NA + NB + (size_t)PL * NB + (size_t)LINES * NA);
+    // twiddles (NA + NB), the rows (PL NB), the axis-1 exchange (LINES NA), the mbarrier
+    static constexpr size_t SMEM =
+        sizeof(float2) * ((size_t)NA + NB + (size_t)PL * NB + (size_t)LINES * NA) + 16;
+    static_assert(R % 2 == 0 && PL >= R && PL >= H1 - R + 1, "cluster slab row split");
 };
 
 __device__ __forceinline__ void cluster_barrier() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n" "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
-// Own box rows k1 in [r0, r0 + rn) of a slab (pitch P1 in HBM) into S.
+// Own box rows k1 in [r0, r0 + rn) of a slab (pitch P1 in HBM) into S, one
+// cp.async.bulk a box column of the rows rounded up to an even count (r0 is
+// even and P1 even, so both ends are 16-byte aligned; the extra bin lies
+// outside the box, or is the padding bin, and is read by no one).
 template <int NB, int P1, int PL>
-__device__ __forceinline__ void load_rows(float2* S, const float2* src, int r0, int rn, int nk2, int b2, int warp,
-                                          int lane) {
-    for (int j = warp; j < nk2; j += kSlabWarps) {
+__device__ __forceinline__ void load_rows(float2* S, const float2* src, int r0, int rn, int nk2, int b2,
+                                          uint64_t* bar, uint32_t& phase, int* status) {
+    const uint32_t bytes = rn > 0 ? (uint32_t)(((rn + 1) & ~1) * sizeof(float2)) : 0u;
+    fence_proxy_async();   // this thread's earlier accesses to S ahead of the copies' writes
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(bar, bytes * (uint32_t)nk2);
+    __syncthreads();
+    if (bytes && (int)threadIdx.x < nk2) {
+        const int j = threadIdx.x;
         const int k2 = j <= b2 ? j : j + (NB - nk2);
-        for (int kl = lane; kl < rn; kl += 32) S[kl + PL * k2] = src[r0 + kl + P1 * k2];
+        bulk_load(S + PL * k2, src + r0 + P1 * k2, bytes, bar);
     }
+    mbar_wait_bounded(bar, phase, status);
+    phase ^= 1;
 }
 
+// Own box rows back to the slab in HBM.  A column's copy covers the rows
+// rounded up to an even count: with rank 0's rows all of [0, R) when the box
+// reaches rank 1 (R even), so no copy writes a bin of the other CTA.
 template <int NB, int P1, int PL>
-__device__ __forceinline__ void store_rows(float2* dst, const float2* S, int r0, int rn, int nk2, int b2, int warp,
-                                           int lane) {
-    for (int j = warp; j < nk2; j += kSlabWarps) {
+__device__ __forceinline__ void store_rows(float2* dst, const float2* S, int r0, int rn, int nk2, int b2) {
+    const uint32_t bytes = rn > 0 ? (uint32_t)(((rn + 1) & ~1) * sizeof(float2)) : 0u;
+    fence_proxy_async();   // this thread's writes of S visible to the copies
+    __syncthreads();
+    if (bytes && (int)threadIdx.x < nk2) {
+        const int j = threadIdx.x;
         const int k2 = j <= b2 ? j : j + (NB - nk2);
-        for (int kl = lane; kl < rn; kl += 32) dst[r0 + kl + P1 * k2] = S[kl + PL * k2];
+        bulk_store(dst + r0 + P1 * k2, S + PL * k2, bytes);
+        bulk_commit();
+        bulk_wait_read();   // S is rewritten by the next unit
     }
+    __syncthreads();
 }
 
 // FFT along axis 2 of the own rows kl < rn; on the inverse, the columns
@@ -169,6 +192,8 @@ struct ClusterCtx {
     float2* X;
     float2* S0;   // the rows of rank 0 and rank 1 (generic addresses)
     float2* S1;
+    uint64_t* bar;
+    uint32_t phase = 0;
     int rank, r0, rn;
     __device__ __forceinline__ ClusterCtx(float2* sm, const SlabArgs& a) {
         cg::cluster_group cl = cg::this_cluster();
@@ -180,7 +205,12 @@ struct ClusterCtx {
         S0 = cl.map_shared_rank(S, 0);
         S1 = cl.map_shared_rank(S, 1);
         r0 = rank * C::R;
-        rn = min(C::R, a.nk1 - r0);
+        rn = min(rank == 0 ? C::R : C::H1 - C::R, a.nk1 - r0);
+        bar = reinterpret_cast<uint64_t*>(X + C::LINES * NA);
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_barrier_init();
+        }
         load_slab_twiddles<NA>(twA, a.twa);
         load_slab_twiddles<NB>(twB, a.twb);
     }
@@ -201,8 +231,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) ns_slab_cluster_inv_kernel(Sl
         const int ch = u / per, ur = u - ch * per;
         const int z = ur / a.n3, s3 = ur - z * a.n3;
         const float2* src = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * (C::P1 * NB);
-        load_rows<NB, C::P1, C::PL>(cx.S, src, cx.r0, cx.rn, a.nk2, a.b2, warp, lane);
-        __syncthreads();
+        load_rows<NB, C::P1, C::PL>(cx.S, src, cx.r0, cx.rn, a.nk2, a.b2, cx.bar, cx.phase, a.status);
         rows_fft<NB, C::PL, true>(cx.S, cx.twB, cx.rn, a.nk2, a.b2, warp, lane);
         cluster_barrier();   // both halves of every column are final
         {
@@ -281,7 +310,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) ns_slab_cluster_fwd_kernel(Sl
         rows_fft<NB, C::PL, false>(cx.S, cx.twB, cx.rn, a.nk2, a.b2, warp, lane);
         __syncthreads();
         float2* dst = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * (C::P1 * NB);
-        store_rows<NB, C::P1, C::PL>(dst, cx.S, cx.r0, cx.rn, a.nk2, a.b2, warp, lane);
+        store_rows<NB, C::P1, C::PL>(dst, cx.S, cx.r0, cx.rn, a.nk2, a.b2);
         cluster_barrier();   // the rows are free for the peer's next unit
     }
 }
@@ -301,8 +330,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) ns_slab_cluster_shrink_kernel
         const int z = ur / a.n3, s3 = ur - z * a.n3;
         float2* slab = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * (C::P1 * NB);
         const float tau = a.tau[a.items[a.item0 + z].s - 1];
-        load_rows<NB, C::P1, C::PL>(cx.S, slab, cx.r0, cx.rn, a.nk2, a.b2, warp, lane);
-        __syncthreads();
+        load_rows<NB, C::P1, C::PL>(cx.S, slab, cx.r0, cx.rn, a.nk2, a.b2, cx.bar, cx.phase, a.status);
         rows_fft<NB, C::PL, true>(cx.S, cx.twB, cx.rn, a.nk2, a.b2, warp, lane);
         cluster_barrier();
         {
@@ -344,7 +372,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) ns_slab_cluster_shrink_kernel
         cluster_barrier();   // every row holds the re-transformed columns
         rows_fft<NB, C::PL, false>(cx.S, cx.twB, cx.rn, a.nk2, a.b2, warp, lane);
         __syncthreads();
-        store_rows<NB, C::P1, C::PL>(slab, cx.S, cx.r0, cx.rn, a.nk2, a.b2, warp, lane);
+        store_rows<NB, C::P1, C::PL>(slab, cx.S, cx.r0, cx.rn, a.nk2, a.b2);
         __syncthreads();   // own rows are reloaded by the next unit (the peer writes them only after the next barrier)
     }
 }
