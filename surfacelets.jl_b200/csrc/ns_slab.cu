@@ -168,11 +168,26 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
         if (z >= nz) break;   // uniform across the CTA
         const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
         const bool wedges = !(mk.low || mk.plain);
+        // a wedge plane over (k1, k2) is constant along the line: one load (the same product, so the
+        // same float32 values as the per-element form)
         float2 v[N1];
+        if (!wedges) {
 #pragma unroll
-        for (int r = 0; r < N1; ++r) {
-            const int i = p + N2 * r;
-            v[r] = wedges ? c_scale(xg[r], mk.wa[i * mk.was] * mk.wb[i * mk.wbs]) : xg[r];
+            for (int r = 0; r < N1; ++r) v[r] = xg[r];
+        } else if (mk.was == 0) {
+            const float a0 = mk.wa[0];
+#pragma unroll
+            for (int r = 0; r < N1; ++r) v[r] = c_scale(xg[r], a0 * mk.wb[(p + N2 * r) * mk.wbs]);
+        } else if (mk.wbs == 0) {
+            const float b0 = mk.wb[0];
+#pragma unroll
+            for (int r = 0; r < N1; ++r) v[r] = c_scale(xg[r], mk.wa[(p + N2 * r) * mk.was] * b0);
+        } else {
+#pragma unroll
+            for (int r = 0; r < N1; ++r) {
+                const int i = p + N2 * r;
+                v[r] = c_scale(xg[r], mk.wa[i * mk.was] * mk.wb[i * mk.wbs]);
+            }
         }
         float2 u[E];
         reg_line_fft_v<N, true>(v, p, xl, tw, u);
