@@ -65,6 +65,13 @@ def test_ranges_reproduce_the_transforms(sfl, dims, pipeline, dtype):
     assert torch.equal(y, yf)
     with pytest.raises(sfl.ArgumentError):
         ops.analyze_range(X, S - 1, 2, ops.new_subbands(2))
+    # spectra move in 16-byte blocks: a spectrum one bin off a 16-byte boundary is refused
+    Xb = torch.empty(ops.nch * ops.spectrum_elems + 1, dtype=torch.complex64, device="cuda")[1:]
+    c1 = sfl.as_colmajor(call[..., :1])
+    for fn in (lambda: ops.forward_spectrum(xd, Xb), lambda: ops.analyze_range(Xb, 0, 1, ops.new_subbands(1)),
+               lambda: ops.accumulate_range(c1, 0, 1, Xb, True), lambda: ops.inverse_spectrum(Xb, y)):
+        with pytest.raises(sfl.ArgumentError, match="16-byte aligned"):
+            fn()
 
 
 def _free_port():
