@@ -178,9 +178,10 @@ int sfl_plan_set_group(sfl_plan* plan, int32_t group);
 
 /* NSSurfacelet kernel pipeline.  All give the same subbands to float32
  * rounding; they differ in speed only.
- *   SLABS (default where supported: axes 1 and 2 of length 64, 96, 128 or
- *     160): a line pass along axis 3 plus one pass per axis-3 slab, skipping
- *     the zero rows and columns of band-limited masks.
+ *   SLABS (default where supported: axes 1 and 2 of length 64, 96, 128, 160
+ *     or 256, axis 3 of length 16, 32, 64, 96, 128, 160 or 256): a line pass
+ *     along axis 3 plus one pass per axis-3 slab, skipping the zero rows and
+ *     columns of band-limited masks.
  *   LINES (default elsewhere): one line pass per axis.
  *   PLANES: a pass along axis 1 plus a 2-D pass per axis-1 frequency plane
  *     (axes 2 and 3 of length 64, 96 or 128).

@@ -735,6 +735,12 @@ bool launch_slab_n(int nb, const SlabArgs& a, int sms, size_t smem, cudaStream_t
         case 96: launch_slab_nn<KIND, NA, 96>(a, sms, smem, st, tag); return true;
         case 128: launch_slab_nn<KIND, NA, 128>(a, sms, smem, st, tag); return true;
         case 160: launch_slab_nn<KIND, NA, 160>(a, sms, smem, st, tag); return true;
+        case 256:
+            if constexpr (NA != 256) {   // 256 x 256 slabs run on clusters (ns_slab_cluster.cu)
+                launch_slab_nn<KIND, NA, 256>(a, sms, smem, st, tag);
+                return true;
+            }
+            return false;
     }
     return false;
 }
@@ -751,11 +757,12 @@ void launch_slab(int na, int nb, const SlabArgs& a, int sms, size_t smem, cudaSt
         case 96: ok = launch_slab_n<KIND, 96>(nb, a, sms, smem, st, tag); break;
         case 128: ok = launch_slab_n<KIND, 128>(nb, a, sms, smem, st, tag); break;
         case 160: ok = launch_slab_n<KIND, 160>(nb, a, sms, smem, st, tag); break;
+        case 256: ok = launch_slab_n<KIND, 256>(nb, a, sms, smem, st, tag); break;
     }
     if (!ok) throw ArgError("no slab kernel for this size");
 }
 
-bool slab_len(int n) { return n == 64 || n == 96 || n == 128 || n == 160; }
+bool slab_len(int n) { return n == 64 || n == 96 || n == 128 || n == 160 || n == 256; }
 
 int slab_pitch(int h1) { return slab_pitch_c(h1); }
 
@@ -1025,7 +1032,9 @@ int chunk_end(const NSPlan& P, int i0) {
 
 bool ns_slab_supported(int n1, int n2, int n3) {
     if (!reg_fft_supported(n3)) return false;
-    return (slab_len(n1) && slab_len(n2) && slab_smem(n1, n2) <= kSlabSmemMax) || slab_cluster_supported(n1, n2);
+    // one CTA a slab where the slab fits its shared memory (two CTAs an SM up to 112 KB, one above),
+    // else two-CTA clusters
+    return (slab_len(n1) && slab_len(n2) && slab_smem(n1, n2) <= kSlabSmemOneCta) || slab_cluster_supported(n1, n2);
 }
 
 // Support box of a table on the rfft grid (h1, n2, n3), k1 fastest.

@@ -11,7 +11,7 @@ namespace sfl {
 
 constexpr int kSlabThreads = 512;
 constexpr int kSlabWarps = kSlabThreads / 32;
-constexpr size_t kSlabSmemMax = 112 * 1024;   // two CTAs an SM
+constexpr size_t kSlabSmemOneCta = 227 * 1024;   // the most one CTA may hold
 
 struct SlabArgs {
     float2* spec;            // padded spectra, item z at spec + z * spec_zstride

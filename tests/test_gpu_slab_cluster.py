@@ -1,7 +1,9 @@
-"""The slab pipeline at 256 x 256 (x n3), where one slab (130 x 256 complex
-bins) is split over the two CTAs of a thread-block cluster: analysis and
-synthesis against the float64 oracle, the line pipeline, the fused denoiser
-and streaming (bit for bit), complex data and the adjoints."""
+"""The slab pipeline with a 256-point axis: at 256 x 256 (x n3) one slab
+(130 x 256 complex bins) is split over the two CTAs of a thread-block
+cluster; with the other axis of 64 to 160 points a slab fits one CTA's
+shared memory.  Analysis and synthesis against the float64 oracle, the line
+pipeline, the fused denoiser and streaming (bit for bit), complex data and
+the adjoints."""
 
 import numpy as np
 import pytest
@@ -94,3 +96,29 @@ def test_cluster_slabs_denoise_and_stream_bit_for_bit(sfl):
     ys = sfl.volume_like(dims)
     sfl.synthesize_(lambda i: c[..., i - 1], ys, ws)
     assert torch.equal(ys, sfl.synthesize(ws, c))
+
+
+@pytest.mark.parametrize("dims", [(256, 128, 32), (128, 256, 16), (256, 160, 16), (96, 256, 16), (256, 64, 32)])
+def test_one_cta_slabs_with_a_256_axis(sfl, dims):
+    import torch
+    kw = dict(scales=2, direction_levels=[1, 2], bernstein_order=6)
+    rng = np.random.default_rng(sum(dims))
+    x = rng.standard_normal(dims).astype(np.float32)
+    t = sfl.NSSurfacelet(**kw)
+    ws = sfl.make_workspace(t, "float32", dims)
+    assert ws.tuning()[0] == "slabs"
+    T = N.make_tables(N.NSParams.make(**kw), dims)
+    xd = sfl.to_device(x)
+    c = sfl.analyze(ws, xd)
+    ch = sfl.to_host(c)
+    assert rel_l2(ch, N.analyze(T, x.astype(np.float64))) <= REL
+    assert rel_l2(sfl.to_host(sfl.synthesize(ws, c)), x) <= REL
+    cr = rng.standard_normal(ch.shape).astype(np.float32)
+    y = sfl.to_host(sfl.synthesize(ws, sfl.to_device(cr)))
+    assert rel_l2(y, N.synthesize(T, cr.astype(np.float64))) <= REL
+    tau = torch.full((ws.nsubbands,), 0.1, device="cuda")
+    ref = sfl.synthesize(ws, sfl.as_colmajor(torch.sign(c) * torch.clamp(c.abs() - tau, min=0)))
+    assert torch.equal(sfl.denoise(ws, xd, tau), ref)
+    import ctypes as C
+    st = C.c_int32(-1)
+    assert sfl.lib.sfl_plan_status(ws._h, C.byref(st), 0) == 0 and st.value == 0
