@@ -524,6 +524,7 @@ def main():
         shrink = lambda i, b: sfl.as_colmajor(torch.nn.functional.softshrink(b, 0.05))
         sfl.analyze_synthesize_stream(lambda i, b: b, yl, xl, wa, wsy)
         pr32 = float(torch.linalg.vector_norm(yl - xl) / torch.linalg.vector_norm(xl))
+        sfl.analyze_synthesize_stream(shrink, yl, xl, wa, wsy)   # warm-up of the thresholding callback
         ms_stream = timed(lambda: sfl.analyze_synthesize_stream(shrink, yl, xl, wa, wsy), 2)
         c32 = sfl.analyze(wa, xl)
         c16, sc16 = sfl.analyze_bf16(wa, xl)

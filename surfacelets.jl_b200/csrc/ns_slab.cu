@@ -126,6 +126,13 @@ template <int N>
 constexpr int mask_minb() { return (N == 96 || N == 160) ? 1 : 2; }
 template <int N>
 constexpr int accum_minb() { return (N == 96 || N == 160 || N >= 256) ? 1 : 2; }
+// Accumulation lengths whose sums go to shared memory (their register form spills).
+template <int N>
+constexpr bool accum_sums_shared() { return N == 96 || N == 128 || N == 160; }
+template <int N>
+constexpr size_t accum_smem() {
+    return RegGeom<N>::SMEM + (accum_sums_shared<N>() ? sizeof(float2) * RegGeom<N>::M * RegGeom<N>::N2 * 256 : 0);
+}
 
 // Analysis line pass over IPC subbands of one mask group per CTA: a line's X
 // times the group factor is loaded once, then per subband scaled by its two
@@ -223,12 +230,22 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
     if (valid) bx.k12(l, k1, k2);
     float2* a = acc + k1 + P1 * k2;
     float2* xl = xch + lp * Ge::XLINE;
-    float2 s[E];
+    // the line's sums: in registers, or (lengths whose registers would spill) in shared memory after
+    // the exchange rows, value q of thread t at [q * 256 + t]
+    constexpr bool kSumsShared = accum_sums_shared<N>();
+    float2 sr[kSumsShared ? 1 : E];
+    float2* ss = xch + LP * Ge::XLINE + tid;
+    auto sum = [&](int q) -> float2& {
+        if constexpr (kSumsShared)
+            return ss[q * Ge::THREADS];
+        else
+            return sr[q];
+    };
 #pragma unroll
     for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
         for (int k = 0; k < N2; ++k)
-            s[j * N2 + k] = valid ? a[((p + N2 * j) + N1 * k) * s3] : make_float2(0.f, 0.f);
+            sum(j * N2 + k) = valid ? a[((p + N2 * j) + N1 * k) * s3] : make_float2(0.f, 0.f);
     const long long si_nat = (long long)tb.h1 * tb.n2;
     const int lnat = k1 + tb.h1 * k2;
     // the group factor of the line (group table, bandpass table or the lowpass factors), once for all items
@@ -256,7 +273,8 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
             for (int k = 0; k < N2; ++k) {
                 const int k3 = (p + N2 * j) + N1 * k;
                 const float m = wedges ? gf[j * N2 + k] * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]) : gf[j * N2 + k];
-                s[j * N2 + k] = c_add(s[j * N2 + k], c_scale(u[j * N2 + k], m));
+                float2& t = sum(j * N2 + k);
+                t = c_add(t, c_scale(u[j * N2 + k], m));
             }
         __syncthreads();   // the exchange rows are reused by the next item
     }
@@ -264,7 +282,7 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
 #pragma unroll
         for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
-            for (int k = 0; k < N2; ++k) a[((p + N2 * j) + N1 * k) * s3] = s[j * N2 + k];
+            for (int k = 0; k < N2; ++k) a[((p + N2 * j) + N1 * k) * s3] = sum(j * N2 + k);
     }
 }
 
@@ -811,13 +829,13 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
     static bool configured = false;
     if (!configured) {
         cuda_check(cudaFuncSetAttribute(ns_slab_accum_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)Ge::SMEM),
+                                        (int)accum_smem<N>()),
                    "cudaFuncSetAttribute");
         configured = true;
     }
     dim3 grid((nlines + Ge::LP - 1) / Ge::LP, nch);
     int tok = prof_begin("ns_slab_accum_axis3", st);
-    ns_slab_accum_kernel<N><<<grid, Ge::THREADS, Ge::SMEM, st>>>(Y, P.SP, nz, P.P1, P.P1 * P.dims[1], bx, P.tb,
+    ns_slab_accum_kernel<N><<<grid, Ge::THREADS, accum_smem<N>(), st>>>(Y, P.SP, nz, P.P1, P.P1 * P.dims[1], bx, P.tb,
                                                                  P.items.as<NSItem>(), i0, synth, acc,
                                                                  P.ffts.at(P.dims[2])->sh.tw, nlines, ychs, achs);
     prof_end(tok, st);
