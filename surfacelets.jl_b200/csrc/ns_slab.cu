@@ -1052,7 +1052,7 @@ bool ns_slab_supported(int n1, int n2, int n3) {
     if (!reg_fft_supported(n3)) return false;
     // one CTA a slab where the slab fits its shared memory (two CTAs an SM up to 112 KB, one above),
     // else two-CTA clusters
-    return (slab_len(n1) && slab_len(n2) && slab_smem(n1, n2) <= kSlabSmemOneCta) || slab_cluster_supported(n1, n2);
+    return (slab_len(n1) && slab_len(n2) && slab_smem(n1, n2) <= kSlabSmemOneCta) || slab_cluster_resident(n1, n2);
 }
 
 // Support box of a table on the rfft grid (h1, n2, n3), k1 fastest.

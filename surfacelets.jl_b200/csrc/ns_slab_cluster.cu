@@ -435,6 +435,38 @@ void launch_nn(int kind, const SlabArgs& a, int sms, cudaStream_t st, const char
 
 bool slab_cluster_supported(int na, int nb) { return na == 256 && nb == 256; }
 
+// Whether a two-CTA cluster of the slab kernels fits the current device (a
+// partitioned or shared device may not offer it); asked once a device.
+bool slab_cluster_resident(int na, int nb) {
+    if (!slab_cluster_supported(na, nb)) return false;
+    static int cached[64];   // 0 unknown, 1 yes, 2 no
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return false;
+    if (cached[dev] == 0) {
+        using C = ClusterSlab<256, 256>;
+        auto kern = ns_slab_cluster_inv_kernel<256, 256, 1>;
+        int n = 0;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM) == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = kClusterCTAs;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(kClusterCTAs);
+            cfg.blockDim = dim3(kSlabThreads);
+            cfg.dynamicSmemBytes = C::SMEM;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) n = 0;
+        }
+        cudaGetLastError();   // a refused query leaves no sticky error behind
+        cached[dev] = n > 0 ? 1 : 2;
+    }
+    return cached[dev] == 1;
+}
+
 bool launch_slab_cluster(int kind, int na, int nb, const SlabArgs& a, int sms, cudaStream_t st, const char* tag) {
     if (na == 256 && nb == 256) {
         static_assert(ClusterSlab<256, 256>::SMEM <= 227 * 1024, "cluster slab exceeds shared memory");

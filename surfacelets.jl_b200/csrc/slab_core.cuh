@@ -113,5 +113,6 @@ __device__ __forceinline__ int pair_subline(int s) {
 // when (na, nb) has none.
 bool launch_slab_cluster(int kind, int na, int nb, const SlabArgs& a, int sms, cudaStream_t st, const char* tag);
 bool slab_cluster_supported(int na, int nb);
+bool slab_cluster_resident(int na, int nb);
 
 }  // namespace sfl
