@@ -343,6 +343,17 @@ def main():
         "kernel_algorithmic_gbs": {k: tag_bytes[k] / (v[0] / 1e3) / 1e9 for k, v in per_tag.items()
                                    if tag_bytes.get(k)},
     }
+    # The co-limit: FP32 FFT arithmetic on the CUDA cores.  Algorithmic FLOPs
+    # are the reference's unpruned cascade, 2.5 N log2 N a real 3-D FFT and
+    # (1 + S) FFTs an operator, three operators a volume; the peak is the
+    # nominal FMA rate (148 SMs x 128 lanes x 2 FLOP) at the sampled SM clock.
+    mhz = clk["sm_mhz"] if clk else 1965.0
+    fft_flop = 3.0 * (1 + S) * 2.5 * N * np.log2(N) * B * world
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    fp32_ach = fft_flop / (ms / 1e3) / 1e12 / world
+    line["fp32_roofline"] = {"bound": "fp32", "algorithmic_flop_per_voxel": fft_flop / (N * B * world),
+                             "achieved": fp32_ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                             "frac": fp32_ach / fp32_peak, "peak_kind": "nominal at the sampled SM clock"}
     if clk:
         line["clocks"] = {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}
 
