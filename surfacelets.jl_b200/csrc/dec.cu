@@ -13,6 +13,7 @@
 //   vector.  The coarse lowpass is Re(bfft(C))/|C|.
 // Inverse: the mirror image, with one kernel that forms the Hermitian sum of
 // the three hourglasses over the full grid.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -171,6 +172,113 @@ __global__ void irc_stage_kernel(float2* S, int h0, int h1, int h2, int K, int m
         }
         S[aA] = nA;
         S[aB] = nB;
+    }
+}
+
+// Every IRC stage of hourglass K on one plane k_K of S_K (the plane over the
+// two transverse axes), held in shared memory: one HBM round trip for the
+// whole cascade instead of one per stage.  The analysis form applies the
+// hourglass mask on load (S_K = X[half_K] V_K s, as hg_mask_kernel) and runs
+// the stages in order; the synthesis form runs them in reverse with the
+// synthesis filters.  Per stage the same butterfly, in the same order of
+// operations, as irc_stage_kernel.  One CTA a plane (blockIdx.x = k_K).
+constexpr int kIrcPlaneMaxStages = 8;
+constexpr int kIrcPlaneThreads = 1024;
+constexpr int kIrcPlaneBatch = 4;
+struct IrcPlaneStages {
+    int n;
+    int m[kIrcPlaneMaxStages], b[kIrcPlaneMaxStages];
+    const float2* f0[kIrcPlaneMaxStages];
+    const float2* f1[kIrcPlaneMaxStages];
+};
+
+template <bool SYNTH>
+__global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(float2* S, int h0, int h1, int h2, int K, IrcPlaneStages sg,
+                                                        const float2* __restrict__ X, int n0, int n1,
+                                                        const float* __restrict__ V, float s) {
+    extern __shared__ float2 pl[];
+    const int hd[3] = {h0, h1, h2};
+    const long long str[3] = {1, h0, (long long)h0 * h1};
+    const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
+    const int a1 = hd[m1], a2 = hd[m2];
+    const int kK = blockIdx.x;
+    const long long base = (long long)kK * str[K];
+    const int tot = a1 * a2;
+    // kIrcPlaneBatch independent loads in flight per thread (one CTA an SM holds the plane)
+    for (int q0 = threadIdx.x; q0 < tot; q0 += kIrcPlaneBatch * blockDim.x) {
+        float2 v[kIrcPlaneBatch];
+#pragma unroll
+        for (int u = 0; u < kIrcPlaneBatch; ++u) {
+            const int q = q0 + u * blockDim.x;
+            v[u] = make_float2(0.f, 0.f);
+            if (q < tot) {
+                const int i1 = q % a1, i2 = q / a1;
+                const long long g = base + i1 * str[m1] + i2 * str[m2];
+                if (!SYNTH) {
+                    int c[3];
+                    c[K] = kK;
+                    c[m1] = i1;
+                    c[m2] = i2;
+                    v[u] = c_scale(X[lin3(c[0], c[1], c[2], n0, n1)], V[g] * s);
+                } else {
+                    v[u] = S[g];
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kIrcPlaneBatch; ++u) {
+            const int q = q0 + u * blockDim.x;
+            if (q < tot) pl[q] = v[u];
+        }
+    }
+    __syncthreads();
+    const int nKh = hd[K];
+    for (int t = 0; t < sg.n; ++t) {
+        const int u = SYNTH ? sg.n - 1 - t : t;
+        const int b = sg.b[u];
+        const bool first = sg.m[u] == m1;
+        const int half = (first ? a1 : a2) / 2;
+        const int npairs = half * (first ? a2 : a1);
+        // the stage's filter row at k_K (over the stage's axis) into shared memory
+        const int am = first ? a1 : a2;
+        float2* cf = pl + tot;
+        for (int i = threadIdx.x; i < am; i += blockDim.x) {
+            cf[i] = sg.f0[u][kK + (long long)nKh * i];
+            cf[am + i] = sg.f1[u][kK + (long long)nKh * i];
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < npairs; q += blockDim.x) {
+            // consecutive threads on consecutive words of the plane: the pair index runs fastest along
+            // the first axis, the other index along the second
+            int pq, o;
+            if (first) {
+                pq = q % half;
+                o = q / half;
+            } else {
+                o = q % a1;
+                pq = q / a1;
+            }
+            const int cA = (pq / b) * 2 * b + (pq % b), cB = cA + b;
+            const int qA = first ? cA + a1 * o : o + a1 * cA;
+            const int qB = first ? cB + a1 * o : o + a1 * cB;
+            const float2 A = pl[qA], Bv = pl[qB];
+            const float2 f0A = cf[cA], f0B = cf[cB], f1A = cf[am + cA], f1B = cf[am + cB];
+            float2 nA, nB;
+            if (!SYNTH) {
+                nA = c_add(c_mul(f0A, A), c_mul(f0B, Bv));
+                nB = c_add(c_mul(f1A, A), c_mul(f1B, Bv));
+            } else {
+                nA = c_add(c_mul(f0A, A), c_mul(f1A, Bv));
+                nB = c_add(c_mul(f0B, A), c_mul(f1B, Bv));
+            }
+            pl[qA] = nA;
+            pl[qB] = nB;
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < tot; q += blockDim.x) {
+        const int i1 = q % a1, i2 = q / a1;
+        S[base + i1 * str[m1] + i2 * str[m2]] = pl[q];
     }
 }
 
@@ -626,6 +734,43 @@ void pyr_merge(DecPlan& D, int j, cudaStream_t st, bool adjoint = false) {
     cuda_check(cudaGetLastError(), "pyr_merge_kernel");
 }
 
+// The fused plane pass holds one k_K plane of S_K (n_m1 x n_m2 complex values)
+// and one stage's two filter rows in shared memory: up to 227 KB, and at most
+// kIrcPlaneMaxStages stages.
+size_t irc_plane_smem(const DecLevelDev& L, int K) {
+    const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
+    const int a1 = L.hd[K][m1], a2 = L.hd[K][m2];
+    return sizeof(float2) * ((size_t)a1 * a2 + 2 * (size_t)std::max(a1, a2));   // the plane + a stage's filter row
+}
+
+bool irc_plane_fits(const DecLevelDev& L, int K) {
+    return irc_plane_smem(L, K) <= 227 * 1024 && L.stages[K].size() <= (size_t)kIrcPlaneMaxStages;
+}
+
+IrcPlaneStages irc_plane_stages(const DecLevelDev& L, int K, bool synth) {
+    IrcPlaneStages ps{};
+    ps.n = (int)L.stages[K].size();
+    for (int t = 0; t < ps.n; ++t) {
+        const DecStageDev& sg = L.stages[K][t];
+        ps.m[t] = sg.m;
+        ps.b[t] = sg.b;
+        ps.f0[t] = sg.f[synth ? 2 : 0].as<float2>();
+        ps.f1[t] = sg.f[synth ? 3 : 1].as<float2>();
+    }
+    return ps;
+}
+
+template <bool SYNTH>
+void irc_plane_configure(size_t smem) {
+    static size_t configured = 0;
+    if (smem > configured) {
+        cuda_check(cudaFuncSetAttribute(irc_plane_kernel<SYNTH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem),
+                   "cudaFuncSetAttribute(irc_plane)");
+        configured = smem;
+    }
+}
+
 void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
     const float2* X = D.spectra[j]->as<float2>();
@@ -636,21 +781,32 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
         for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
         float s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
         long long tot = (long long)hd[0] * hd[1] * hd[2];
-        {
+        if (irc_plane_fits(L, K)) {
+            // mask and every stage in one pass over the k_K planes
+            IrcPlaneStages ps = irc_plane_stages(L, K, false);
+            const size_t smem = irc_plane_smem(L, K);
+            irc_plane_configure<false>(smem);
+            int tok = prof_begin("dec_irc_plane", st);
+            irc_plane_kernel<false><<<hd[K], kIrcPlaneThreads, smem, st>>>(S, hd[0], hd[1], hd[2], K, ps, X, L.n[0], L.n[1],
+                                                              L.V[K].as<float>(), s);
+            prof_end(tok, st);
+            cuda_check(cudaGetLastError(), "irc_plane_kernel");
+        } else {
             int tok = prof_begin("dec_hg_mask", st);
             hg_mask_kernel<<<grid_for(tot), 256, 0, st>>>(X, L.n[0], L.n[1], S, hd[0], hd[1], hd[2], L.V[K].as<float>(), s);
             prof_end(tok, st);
-        }
-        cuda_check(cudaGetLastError(), "hg_mask_kernel");
-        for (auto& sg : L.stages[K]) {
-            long long pairs = tot / 2;
-            {
-                int tok = prof_begin("dec_irc", st);
-                irc_stage_kernel<<<grid_for(pairs), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
-                                                                  sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0, 0);
-                prof_end(tok, st);
+            cuda_check(cudaGetLastError(), "hg_mask_kernel");
+            for (auto& sg : L.stages[K]) {
+                long long pairs = tot / 2;
+                {
+                    int tok = prof_begin("dec_irc", st);
+                    irc_stage_kernel<<<grid_for(pairs), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                                                                      sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0,
+                                                                      0);
+                    prof_end(tok, st);
+                }
+                cuda_check(cudaGetLastError(), "irc_stage_kernel");
             }
-            cuda_check(cudaGetLastError(), "irc_stage_kernel");
         }
         for (int m = 0; m < 3; ++m)
             if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], true, st);
@@ -686,15 +842,30 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
         for (int m = 0; m < 3; ++m)
             if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
         long long tot = (long long)hd[0] * hd[1] * hd[2];
-        for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
-            auto& sg = L.stages[K][s];
-            {
-                int tok = prof_begin("dec_irc", st);
-                irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
-                                                                    sg.f[2].as<float2>(), sg.f[3].as<float2>(), 1, 0);
+        if (irc_plane_fits(L, K)) {
+            // every stage, in reverse, in one pass over the k_K planes
+            if (!L.stages[K].empty()) {
+                IrcPlaneStages ps = irc_plane_stages(L, K, true);
+                const size_t smem = irc_plane_smem(L, K);
+                irc_plane_configure<true>(smem);
+                int tok = prof_begin("dec_irc_plane", st);
+                irc_plane_kernel<true><<<hd[K], kIrcPlaneThreads, smem, st>>>(S, hd[0], hd[1], hd[2], K, ps, nullptr, 0, 0,
+                                                                 nullptr, 1.f);
                 prof_end(tok, st);
+                cuda_check(cudaGetLastError(), "irc_plane_kernel");
             }
-            cuda_check(cudaGetLastError(), "irc_stage_kernel");
+        } else {
+            for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
+                auto& sg = L.stages[K][s];
+                {
+                    int tok = prof_begin("dec_irc", st);
+                    irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                                                                        sg.f[2].as<float2>(), sg.f[3].as<float2>(), 1,
+                                                                        0);
+                    prof_end(tok, st);
+                }
+                cuda_check(cudaGetLastError(), "irc_stage_kernel");
+            }
         }
         ha.S[K] = S;
         ha.V[K] = L.V[K].as<float>();
