@@ -54,6 +54,9 @@ CASES = [
     ((32, 32, 32), 2, 1, [np.array([[-1, 2, 0], [1, -1, 1], [0, 3, -1]])], 6),
     ((24, 24, 24), 1.5, 1, [0], 12),
     ((128, 128, 128), 2, 3, [2, 2, 3], 12),
+    # hourglass 3's finest plane (256 x 128 complex, 256 KB) exceeds shared memory and takes the
+    # per-stage IRC kernels; every other plane takes the fused plane pass
+    ((256, 128, 32), 2, 2, [1, 2], 8),
 ]
 
 
