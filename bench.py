@@ -166,6 +166,65 @@ def kernel_bytes(tag, P, launches_per_step, nz_total):
     return per_item * nz_total + extra * launches_per_step
 
 
+def run_decimated(args):
+    """The decimated Surfacelet(scales=3, direction_levels=[2,2,3], pyramid_ratio=2) alone:
+    analyze + synthesize of a batch of float32 volumes as plain calls on one workspace.  This is
+    the workload of its launch list and kernel captures; it prints one JSON line with the step time
+    and the per-kernel CUDA-event times of a profiled replay (the headline stays the default
+    NSSurfacelet workload)."""
+    import ctypes as C
+
+    import torch
+    torch.cuda.set_device(0)
+    sfl = load_package()
+    lib = sfl.lib
+    B = args.batch
+    N = int(np.prod(DIMS))
+    wd = sfl.make_workspace(sfl.Surfacelet(**DEC_KW), "float32", DIMS)
+    gen = torch.Generator(device="cuda").manual_seed(1234)
+    xs = [sfl.volume_like(DIMS).copy_(torch.randn(DIMS, device="cuda", generator=gen)) for _ in range(B)]
+    cds = [torch.empty(wd.ncoeffs, device="cuda") for _ in range(B)]
+    yds = [sfl.volume_like(DIMS) for _ in range(B)]
+
+    def step():
+        for b in range(B):
+            sfl.analyze_(cds[b], wd, xs[b])
+            sfl.synthesize_(yds[b], wd, cds[b])
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    rel = float(torch.linalg.vector_norm(yds[0] - xs[0]) / torch.linalg.vector_norm(xs[0]))
+    lib.sfl_profile_reset()
+    lib.sfl_profile_enable(1)
+    step()
+    torch.cuda.synchronize()
+    lib.sfl_profile_enable(0)
+    buf = C.create_string_buffer(8192)
+    lib.sfl_profile_tags(buf, 8192)
+    kernels = {}
+    for tg in [v for v in buf.value.decode().split("\n") if v]:
+        tot, cnt = C.c_double(), C.c_int64()
+        lib.sfl_profile_read(tg.encode(), C.byref(tot), C.byref(cnt))
+        kernels[tg] = {"ms_per_step": tot.value, "launches_per_step": cnt.value}
+    lib.sfl_profile_reset()
+    r = DEC_KW["pyramid_ratio"]
+    print(json.dumps({
+        "metric": "Mvoxels/s analyze+synthesize", "value": B * N / (ms / 1e3) / 1e6, "unit": "Mvoxels/s",
+        "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"Surfacelet(scales=3, direction_levels=[2,2,3], pyramid_ratio={r}) "
+                               + "x".join(str(d) for d in DIMS) + " float32, analyze+synthesize, plain calls",
+                   "batch": B},
+        "perfect_reconstruction_rel_l2": rel, "kernels": kernels}))
+
+
 def main():
     global DIMS, NS_KW
     ap = argparse.ArgumentParser()
@@ -181,6 +240,8 @@ def main():
                     help="volume size (a smaller or larger case for profiling; the extra lines need the default)")
     ap.add_argument("--levels", type=int, nargs="+", default=NS_KW["direction_levels"],
                     help="direction levels per scale (scales = their count)")
+    ap.add_argument("--workload", default="ns", choices=["ns", "decimated"],
+                    help="decimated: the decimated Surfacelet 128^3 alone, for its profiles (not the headline)")
     ap.add_argument("--mode", default="graph", choices=["graph", "calls"],
                     help="graph: the batch as one CUDA graph over up to 4 workspaces (sfl_batch_*); "
                          "calls: a loop of plain calls on one workspace")
@@ -195,6 +256,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "decimated":
+        DIMS = tuple(args.dims)
+        run_decimated(args)
         return
 
     import torch

@@ -192,17 +192,45 @@ struct IrcPlaneStages {
     const float2* f1[kIrcPlaneMaxStages];
 };
 
+// The planes of up to three hourglasses in one launch: job t owns the CTAs
+// [first, first + hd[K]) (one per k_K plane); the hourglasses' S_K are
+// separate buffers.
+struct IrcPlaneJob {
+    float2* S;
+    int K, first;
+    int hd[3];
+    const float* V;   // analysis: the hourglass mask V_K and the subband scale s
+    float s;
+    IrcPlaneStages sg;
+};
+struct IrcPlaneJobs {
+    int n;
+    IrcPlaneJob job[3];
+};
+
 template <bool SYNTH>
-__global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(float2* S, int h0, int h1, int h2, int K, IrcPlaneStages sg,
-                                                        const float2* __restrict__ X, int n0, int n1,
-                                                        const float* __restrict__ V, float s) {
+__global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJobs jobs, const float2* __restrict__ X,
+                                                                     int n0, int n1) {
     extern __shared__ float2 pl[];
-    const int hd[3] = {h0, h1, h2};
-    const long long str[3] = {1, h0, (long long)h0 * h1};
-    const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
-    const int a1 = hd[m1], a2 = hd[m2];
-    const int kK = blockIdx.x;
-    const long long base = (long long)kK * str[K];
+    int t0 = 0;
+    while (t0 + 1 < jobs.n && (int)blockIdx.x >= jobs.job[t0 + 1].first) ++t0;
+    const IrcPlaneJob& jb = jobs.job[t0];
+    float2* S = jb.S;
+    const int K = jb.K;
+    const float* __restrict__ V = jb.V;
+    const float s = jb.s;
+    const IrcPlaneStages& sg = jb.sg;
+    // extents and strides of the hourglass axis K and the transverse axes m1 < m2, as scalars
+    const int h0 = jb.hd[0], h1 = jb.hd[1], h2 = jb.hd[2];
+    const long long p1 = h0, p2 = (long long)h0 * h1;   // S_K strides of axes 1, 2
+    const long long x1 = n0, x2 = (long long)n0 * n1;   // X strides of axes 1, 2
+    const int nKh = K == 0 ? h0 : (K == 1 ? h1 : h2);
+    const int a1 = K == 0 ? h1 : h0, a2 = K == 2 ? h1 : h2;
+    const long long sK = K == 0 ? 1 : (K == 1 ? p1 : p2), s1 = K == 0 ? p1 : 1, s2 = K == 2 ? p1 : p2;
+    const long long xK = K == 0 ? 1 : (K == 1 ? x1 : x2), xa = K == 0 ? x1 : 1, xb = K == 2 ? x1 : x2;
+    const int kK = blockIdx.x - jb.first;
+    const long long base = (long long)kK * sK;
+    const long long xbase = (long long)kK * xK;
     const int tot = a1 * a2;
     // kIrcPlaneBatch independent loads in flight per thread (one CTA an SM holds the plane)
     for (int q0 = threadIdx.x; q0 < tot; q0 += kIrcPlaneBatch * blockDim.x) {
@@ -213,13 +241,9 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(float2* S, 
             v[u] = make_float2(0.f, 0.f);
             if (q < tot) {
                 const int i1 = q % a1, i2 = q / a1;
-                const long long g = base + i1 * str[m1] + i2 * str[m2];
+                const long long g = base + i1 * s1 + i2 * s2;
                 if (!SYNTH) {
-                    int c[3];
-                    c[K] = kK;
-                    c[m1] = i1;
-                    c[m2] = i2;
-                    v[u] = c_scale(X[lin3(c[0], c[1], c[2], n0, n1)], V[g] * s);
+                    v[u] = c_scale(X[xbase + i1 * xa + i2 * xb], V[g] * s);
                 } else {
                     v[u] = S[g];
                 }
@@ -232,11 +256,10 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(float2* S, 
         }
     }
     __syncthreads();
-    const int nKh = hd[K];
     for (int t = 0; t < sg.n; ++t) {
         const int u = SYNTH ? sg.n - 1 - t : t;
         const int b = sg.b[u];
-        const bool first = sg.m[u] == m1;
+        const bool first = sg.m[u] == (K == 0 ? 1 : 0);   // along the plane's first axis m1
         const int half = (first ? a1 : a2) / 2;
         const int npairs = half * (first ? a2 : a1);
         // the stage's filter row at k_K (over the stage's axis) into shared memory
@@ -278,7 +301,7 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(float2* S, 
     }
     for (int q = threadIdx.x; q < tot; q += blockDim.x) {
         const int i1 = q % a1, i2 = q / a1;
-        S[base + i1 * str[m1] + i2 * str[m2]] = pl[q];
+        S[base + i1 * s1 + i2 * s2] = pl[q];
     }
 }
 
@@ -771,9 +794,42 @@ void irc_plane_configure(size_t smem) {
     }
 }
 
+// One launch of the plane pass over the hourglasses of level L whose plane
+// fits (analysis: with the mask on load from the level spectrum X; synthesis:
+// hourglasses without stages have nothing to do).
+template <bool SYNTH>
+void irc_plane_launch(DecPlan& D, DecLevelDev& L, const float2* X, cudaStream_t st) {
+    IrcPlaneJobs jobs{};
+    size_t smem = 0;
+    int blocks = 0;
+    for (int K = 0; K < 3; ++K) {
+        if (!irc_plane_fits(L, K) || (SYNTH && L.stages[K].empty())) continue;
+        IrcPlaneJob& jb = jobs.job[jobs.n++];
+        jb.S = D.S[K].as<float2>();
+        jb.K = K;
+        jb.first = blocks;
+        for (int d = 0; d < 3; ++d) jb.hd[d] = L.hd[K][d];
+        jb.V = L.V[K].as<float>();
+        int sb[3];
+        for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
+        jb.s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
+        jb.sg = irc_plane_stages(L, K, SYNTH);
+        blocks += L.hd[K][K];
+        smem = std::max(smem, irc_plane_smem(L, K));
+    }
+    if (jobs.n == 0) return;
+    irc_plane_configure<SYNTH>(smem);
+    int tok = prof_begin("dec_irc_plane", st);
+    irc_plane_kernel<SYNTH><<<blocks, kIrcPlaneThreads, smem, st>>>(jobs, X, L.n[0], L.n[1]);
+    prof_end(tok, st);
+    cuda_check(cudaGetLastError(), "irc_plane_kernel");
+}
+
 void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
     const float2* X = D.spectra[j]->as<float2>();
+    // mask and every stage of each hourglass whose plane fits: one pass over the k_K planes of all three
+    irc_plane_launch<false>(D, L, X, st);
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
         float2* S = D.S[K].as<float2>();
@@ -781,17 +837,7 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
         for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
         float s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
         long long tot = (long long)hd[0] * hd[1] * hd[2];
-        if (irc_plane_fits(L, K)) {
-            // mask and every stage in one pass over the k_K planes
-            IrcPlaneStages ps = irc_plane_stages(L, K, false);
-            const size_t smem = irc_plane_smem(L, K);
-            irc_plane_configure<false>(smem);
-            int tok = prof_begin("dec_irc_plane", st);
-            irc_plane_kernel<false><<<hd[K], kIrcPlaneThreads, smem, st>>>(S, hd[0], hd[1], hd[2], K, ps, X, L.n[0], L.n[1],
-                                                              L.V[K].as<float>(), s);
-            prof_end(tok, st);
-            cuda_check(cudaGetLastError(), "irc_plane_kernel");
-        } else {
+        if (!irc_plane_fits(L, K)) {
             int tok = prof_begin("dec_hg_mask", st);
             hg_mask_kernel<<<grid_for(tot), 256, 0, st>>>(X, L.n[0], L.n[1], S, hd[0], hd[1], hd[2], L.V[K].as<float>(), s);
             prof_end(tok, st);
@@ -842,19 +888,7 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
         for (int m = 0; m < 3; ++m)
             if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
         long long tot = (long long)hd[0] * hd[1] * hd[2];
-        if (irc_plane_fits(L, K)) {
-            // every stage, in reverse, in one pass over the k_K planes
-            if (!L.stages[K].empty()) {
-                IrcPlaneStages ps = irc_plane_stages(L, K, true);
-                const size_t smem = irc_plane_smem(L, K);
-                irc_plane_configure<true>(smem);
-                int tok = prof_begin("dec_irc_plane", st);
-                irc_plane_kernel<true><<<hd[K], kIrcPlaneThreads, smem, st>>>(S, hd[0], hd[1], hd[2], K, ps, nullptr, 0, 0,
-                                                                 nullptr, 1.f);
-                prof_end(tok, st);
-                cuda_check(cudaGetLastError(), "irc_plane_kernel");
-            }
-        } else {
+        if (!irc_plane_fits(L, K)) {
             for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
                 auto& sg = L.stages[K][s];
                 {
@@ -870,6 +904,8 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
         ha.S[K] = S;
         ha.V[K] = L.V[K].as<float>();
     }
+    // every stage, in reverse, of each hourglass whose plane fits: one pass over the k_K planes of all three
+    irc_plane_launch<true>(D, L, nullptr, st);
     long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
     {
         int tok = prof_begin("dec_herm_sum", st);
