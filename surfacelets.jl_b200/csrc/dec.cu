@@ -660,8 +660,9 @@ void ifft_full_real(DecPlan& D, float2* X, const int d[3], float* out, int es, f
     launch_pass(l0, s0, f0->sh, g0.nlines, 1, true, st, "dec_fft_real");
 }
 
-// Segmented FFTs along axis m of a half-K spectrum: blocks of length bl.
-void block_fft(DecPlan& D, float2* S, const int hd[3], int m, int bl, bool inv, cudaStream_t st) {
+// Lines of the segmented FFTs along axis m of a half-K spectrum (dims hd):
+// blocks of length bl.
+Lines block_lines(const int hd[3], int m, int bl) {
     long long str[3] = {1, hd[0], (long long)hd[0] * hd[1]};
     int o[2], k = 0;
     for (int d = 0; d < 3; ++d)
@@ -674,6 +675,12 @@ void block_fft(DecPlan& D, float2* S, const int hd[3], int m, int bl, bool inv, 
     g.s2 = (long long)bl * str[m];
     g.si = str[m];
     g.nlines = hd[o[0]] * hd[o[1]] * (hd[m] / bl);
+    return g;
+}
+
+// Segmented FFTs along axis m of a half-K spectrum: blocks of length bl.
+void block_fft(DecPlan& D, float2* S, const int hd[3], int m, int bl, bool inv, cudaStream_t st) {
+    const Lines g = block_lines(hd, m, bl);
     FFTLen* f = get_fft(D.ffts, bl);
     bool tf = g.si != 1;
     bool done = inv ? launch_reg<true>(bl, RLoadC{S, ZMap{}, g}, RStoreC{S, ZMap{}, g}, f->sh.tw, g.nlines, 1, tf, st,
@@ -684,6 +691,98 @@ void block_fft(DecPlan& D, float2* S, const int hd[3], int m, int bl, bool inv, 
     LoadC ld{S, ZMap{}, g, 1.f};
     StoreC sto{S, ZMap{}, g, 1.f};
     launch_pass(ld, sto, f->sh, g.nlines, 1, inv, st, "dec_block_fft");
+}
+
+// Block FFTs of several spectra in one register pass: item z (grid.y) has its
+// own spectrum and line geometry (same length); lines past an item's count
+// read zeros and store nothing.
+constexpr int kMaxLineJobs = 6;
+struct LineJobs {
+    int n = 0;
+    float2* base[kMaxLineJobs];
+    Lines g[kMaxLineJobs];
+};
+struct RLoadCJobs {
+    LineJobs j;
+    struct Ctx {
+        const float2* p;
+        long long si;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const {
+        const bool ok = valid && l < j.g[z].nlines;
+        return Ctx{ok ? j.base[z] + j.g[z].base(l) : nullptr, j.g[z].si};
+    }
+    __device__ __forceinline__ float2 get(const Ctx& c, int i) const {
+        return c.p ? c.p[(long long)i * c.si] : make_float2(0.f, 0.f);
+    }
+};
+struct RStoreCJobs {
+    static constexpr bool kStaged = false;
+    LineJobs j;
+    struct Ctx {
+        float2* p;
+        long long si;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const {
+        const bool ok = valid && l < j.g[z].nlines;
+        return Ctx{ok ? j.base[z] + j.g[z].base(l) : nullptr, j.g[z].si};
+    }
+    __device__ __forceinline__ void put(const Ctx& c, int k, float2 v) const {
+        if (c.p) c.p[(long long)k * c.si] = v;
+    }
+};
+
+// The block FFTs of every hourglass of level L along both transverse axes,
+// grouped into one launch per (block length, line layout); lengths without a
+// register pass run one segmented pass per spectrum and axis.
+void block_fft_level(DecPlan& D, DecLevelDev& L, bool inv, cudaStream_t st) {
+    struct Item {
+        int K, m, bl;
+        bool tf;
+        bool done;
+    };
+    Item items[6];
+    int ni = 0;
+    for (int K = 0; K < 3; ++K)
+        for (int m = 0; m < 3; ++m)
+            if (m != K) items[ni++] = Item{K, m, L.bsize[K][m], m != 0, false};
+    for (int a = 0; a < ni; ++a) {
+        if (items[a].done) continue;
+        LineJobs jobs;
+        int member[kMaxLineJobs];   // the item of each job
+        int nlines = 0;
+        bool inGroup[3] = {false, false, false};
+        for (int b = a; b < ni; ++b) {
+            if (items[b].done || items[b].bl != items[a].bl || items[b].tf != items[a].tf) continue;
+            const int K = items[b].K;
+            // one job per spectrum in a launch (the two axes of S_K would race), and the axes of an
+            // hourglass in their order
+            bool earlier_pending = false;
+            for (int c = 0; c < b; ++c)
+                if (items[c].K == K && !items[c].done) earlier_pending = true;
+            if (inGroup[K] || earlier_pending) continue;
+            inGroup[K] = true;
+            member[jobs.n] = b;
+            jobs.base[jobs.n] = D.S[K].as<float2>();
+            jobs.g[jobs.n] = block_lines(L.hd[K], items[b].m, items[b].bl);
+            nlines = std::max(nlines, jobs.g[jobs.n].nlines);
+            ++jobs.n;
+            items[b].done = true;
+        }
+        const int bl = items[a].bl;
+        FFTLen* f = get_fft(D.ffts, bl);
+        const bool ok = inv ? launch_reg<true>(bl, RLoadCJobs{jobs}, RStoreCJobs{jobs}, f->sh.tw, nlines, jobs.n,
+                                               items[a].tf, st, "dec_block_fft")
+                            : launch_reg<false>(bl, RLoadCJobs{jobs}, RStoreCJobs{jobs}, f->sh.tw, nlines, jobs.n,
+                                                items[a].tf, st, "dec_block_fft");
+        if (!ok) {
+            // no register pass for this length: one generic segmented pass per spectrum and axis
+            for (int t = 0; t < jobs.n; ++t) {
+                const Item& it = items[member[t]];
+                block_fft(D, jobs.base[t], L.hd[it.K], it.m, bl, inv, st);
+            }
+        }
+    }
 }
 
 BlockMap block_map(const DecLevelDev& L, int K) {
@@ -854,8 +953,11 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
                 cuda_check(cudaGetLastError(), "irc_stage_kernel");
             }
         }
-        for (int m = 0; m < 3; ++m)
-            if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], true, st);
+    }
+    // the block FFTs of all three hourglasses, grouped by length and layout
+    block_fft_level(D, L, true, st);
+    for (int K = 0; K < 3; ++K) {
+        float2* S = D.S[K].as<float2>();
         Lines gk = k_lines(L, K);
         FFTLen* f = get_fft(D.ffts, L.n[K]);
         BlockMap bm = block_map(L, K);
@@ -885,8 +987,12 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
             StoreHalfPair sto{S, ZMap{}, gk};
             launch_pass(ld, sto, f->sh, pairs, 1, false, st, "dec_r2c_blocks");
         }
-        for (int m = 0; m < 3; ++m)
-            if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
+    }
+    // the block FFTs of all three hourglasses, grouped by length and layout
+    block_fft_level(D, L, false, st);
+    for (int K = 0; K < 3; ++K) {
+        const int* hd = L.hd[K];
+        float2* S = D.S[K].as<float2>();
         long long tot = (long long)hd[0] * hd[1] * hd[2];
         if (!irc_plane_fits(L, K)) {
             for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
