@@ -166,6 +166,40 @@ def kernel_bytes(tag, P, launches_per_step, nz_total):
     return per_item * nz_total + extra * launches_per_step
 
 
+def host64(t):
+    """A column-major device volume as a float64 NumPy array (Julia axis order)."""
+    return np.asfortranarray(t.permute(*reversed(range(t.dim()))).cpu().numpy().transpose()).astype(np.float64)
+
+
+def oracle_errors(x, c, y, g):
+    """rel. L2 against the float64 oracle of one timed volume's analysis
+    coefficients c = A x, its synthesis y = S c and the adjoint g = S^T y,
+    each streamed subband by subband (host threads for the FFTs)."""
+    sys.path.insert(0, ROOT)
+    from oracle import ns as ON
+    ON.set_fft_workers(os.cpu_count() or 1)
+    try:
+        T = ON.make_tables(ON.NSParams.make(**NS_KW), DIMS)
+        S = c.shape[-1]
+
+        def rel_stream(gen, dev):
+            e2 = r2 = 0.0
+            for s, band in gen:
+                e2 += float(np.sum((host64(dev[..., s - 1]) - band) ** 2))
+                r2 += float(np.sum(band ** 2))
+            return float(np.sqrt(e2 / r2))
+
+        ra = rel_stream(ON.analyze_stream(T, host64(x)), c)
+        yref = ON.synthesize_stream(T, lambda s: host64(c[..., s - 1]))
+        rs = float(np.linalg.norm(host64(y) - yref) / np.linalg.norm(yref))
+        Y = ON.rfft3(host64(y))
+        rg = rel_stream(((s, ON.irfft3(Y * M, DIMS)) for s, M in ON.subband_masks(T, analysis=False)), g)
+    finally:
+        ON.set_fft_workers(1)
+    return {"analyze_rel_l2": ra, "synthesize_rel_l2": rs, "adjoint_synthesize_rel_l2": rg,
+            "volume": "the first volume of the timed batch, all %d subbands" % S}
+
+
 def run_decimated(args):
     """The decimated Surfacelet(scales=3, direction_levels=[2,2,3], pyramid_ratio=2) alone:
     analyze + synthesize of a batch of float32 volumes as plain calls on one workspace.  This is
@@ -337,6 +371,8 @@ def main():
     # correctness of the timed data: perfect reconstruction and A^T = A (tight)
     rel_pr = max(float(torch.linalg.vector_norm(ys[b] - xs[b]) / torch.linalg.vector_norm(xs[b])) for b in range(B))
     rel_adj = float(torch.linalg.vector_norm(gs[0] - cs[0]) / torch.linalg.vector_norm(cs[0]))
+    # and against the float64 oracle: one timed volume's three outputs (rank 0, outside the timed region)
+    vs_oracle = oracle_errors(xs[0], cs[0], ys[0], gs[0]) if rank == 0 else None
 
     # profiled replay: launch counts and per-kernel CUDA-event times
     lib = sfl.lib
@@ -396,7 +432,8 @@ def main():
                    "kernel_times": "CUDA events around every launch, from a replay as plain calls",
                    "l2": "inputs larger than L2 (411 MB of coefficients a volume)"},
         "gpu_launches": launches_per_step * args.steps,
-        "rel_err": {"perfect_reconstruction_rel_l2": rel_pr, "adjoint_vs_analyze_rel_l2": rel_adj},
+        "rel_err": {"perfect_reconstruction_rel_l2": rel_pr, "adjoint_vs_analyze_rel_l2": rel_adj,
+                    "vs_fp64_oracle": vs_oracle},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                      "peak_kind": peak_kind,
@@ -451,7 +488,10 @@ def main():
     e2e_step()
     ms_e2e = timed(e2e_step, max(3, args.steps // 2))
     line["e2e"] = {"value": B * N * world / (ms_e2e / 1e3) / 1e6, "unit": "Mvoxels/s",
-                   "h2d_bytes_per_step": 4 * N * B, "d2h_bytes_per_step": 4 * N * B}
+                   "h2d_bytes_per_step": 4 * N * B, "d2h_bytes_per_step": 4 * N * B,
+                   "scope": "volume in, volume out: each step copies every input volume from pinned host memory "
+                            "and every synthesized volume back; the coefficients (analyze's output and the "
+                            "adjoint's) stay on the device"}
 
     if not args.no_extras and rank == 0:
         # plain unfused single-volume GPU form: the reference's device path
@@ -593,8 +633,10 @@ def main():
         L3 = (256, 256, 256)
         tl = sfl.NSSurfacelet(scales=4, direction_levels=[2, 2, 3, 3])
         wa, wsy = sfl.make_workspace(tl, "float32", L3), sfl.make_workspace(tl, "float32", L3)
-        gl = torch.Generator(device="cuda").manual_seed(256)
-        xl = sfl.volume_like(L3).copy_(torch.randn(L3, device="cuda", generator=gl))
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from phantoms import ellipsoid_phantom
+        xl_host = ellipsoid_phantom(L3, count=24, seed=5)
+        xl = sfl.to_device(xl_host)
         yl = sfl.volume_like(L3)
         # the soft threshold sign(b) max(|b| - 0.05, 0) as one torch kernel (softshrink: the same values)
         shrink = lambda i, b: sfl.as_colmajor(torch.nn.functional.softshrink(b, 0.05))
@@ -608,9 +650,21 @@ def main():
         rel16 = float(torch.linalg.vector_norm(ce - c32) / torch.linalg.vector_norm(c32))
         y16 = sfl.synthesize_bf16(wsy, c16, sc16)
         pr16 = float(torch.linalg.vector_norm(y16 - xl) / torch.linalg.vector_norm(xl))
+        # both coefficient formats against the float64 oracle, streamed subband by subband
+        ON.set_fft_workers(os.cpu_count() or 1)
+        Tl = ON.make_tables(ON.NSParams.make(scales=4, direction_levels=[2, 2, 3, 3]), L3)
+        e32 = e16 = r2 = 0.0
+        for s_, band in ON.analyze_stream(Tl, xl_host.astype(np.float64)):
+            e32 += float(np.sum((host64(c32[..., s_ - 1]) - band) ** 2))
+            e16 += float(np.sum((host64(ce[..., s_ - 1]) - band) ** 2))
+            r2 += float(np.sum(band ** 2))
+        ON.set_fft_workers(1)
         line["large_stream"] = {"workload": "NSSurfacelet(scales=4, direction_levels=[2,2,3,3]) 256^3 float32, S = 73, "
                                             "analysis -> soft threshold -> synthesis one subband at a time",
                                 "value": float(np.prod(L3)) / (ms_stream / 1e3) / 1e6, "unit": "Mvoxels/s",
+                                "input": "ellipsoid phantom: 24 seeded ellipsoids + N(0, 0.05^2)",
+                                "fp32_coefficients_rel_l2_vs_fp64_oracle": float(np.sqrt(e32 / r2)),
+                                "bf16_coefficients_rel_l2_vs_fp64_oracle": float(np.sqrt(e16 / r2)),
                                 "fp32_reconstruction_rel_l2": pr32,
                                 "bf16_coefficients_rel_l2_vs_fp32": rel16,
                                 "bf16_reconstruction_rel_l2": pr16,

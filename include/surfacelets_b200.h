@@ -46,6 +46,7 @@ extern "C" {
 #define SFL_ERR_ALLOC (-4)       /* device memory could not be allocated */
 #define SFL_ERR_STATE (-5)       /* call out of order (streaming) */
 #define SFL_ERR_UNSUPPORTED (-6) /* a size or option this build does not handle */
+#define SFL_ERR_TIMEOUT (-7)     /* a bounded device wait of an earlier call on the plan ran out */
 
 #define SFL_MAX_SCALES 16
 
@@ -167,10 +168,21 @@ int sfl_plan_info(const sfl_plan* plan, int32_t* kind, int32_t dims[3], int32_t*
  * src/transforms/surfacelet.jl:444. */
 int sfl_subband_info(const sfl_plan* plan, int32_t i, int32_t shape[3], int64_t* offset);
 
-/* The plan's device status word, written by kernels whose bounded waits ran
- * out (0 = fine, 1 = a bulk-copy barrier wait timed out).  Synchronizes with
- * the device; reset != 0 clears it.  No counterpart in the reference. */
+/* The plan's status word, written by kernels whose bounded waits ran out
+ * (0 = fine, 1 = a bulk-copy barrier wait timed out).  It lives in mapped
+ * host memory; this call synchronizes with the device first, and reset != 0
+ * clears it.  Every compute call on an NS plan also checks it before
+ * enqueueing anything: a nonzero word is reported once, as SFL_ERR_TIMEOUT
+ * (the word is cleared, the call does nothing; the earlier call's results are
+ * not valid).  No counterpart in the reference. */
 int sfl_plan_status(sfl_plan* plan, int32_t* status, int32_t reset);
+
+/* Self-test of the bounded waits: one kernel waits, with a short iteration
+ * limit, on an mbarrier that nothing completes (no copy in flight), so the
+ * wait runs out and the plan's status word records 1.  The next compute call
+ * on the plan returns SFL_ERR_TIMEOUT once.  NS plans only.  No counterpart
+ * in the reference. */
+int sfl_plan_selftest_wait(sfl_plan* plan, void* stream);
 
 /* Subbands a launch keeps in flight (NS: scratch holds that many spectra).
  * Default 8; only affects speed and scratch size. */

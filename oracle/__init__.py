@@ -12,8 +12,12 @@ Pinning:
   * decimated transform: pinned coefficient-for-coefficient to the SurfBox
     golden fingerprints that the reference's own test suite carries
     (test/reference/surfbox_irc.{bin,txt}, re-encoded under tests/golden/);
-  * nonsubsampled transform: the reference ships no golden coefficients, so it
-    is pinned through the reference's component and property tests
+  * nonsubsampled transform: the reference ships no golden coefficients; its
+    hourglass and NDFB banks are pinned to the SurfBox golden data the
+    reference's suite carries for them (test/reference/surfbox_hourglass_32.bin
+    and surfbox_directions_32.bin: the hourglass partition and the 12-wedge
+    direction partition, re-encoded under tests/golden/), and the whole
+    transform through the reference's component and property tests
     (partition of unity, Parseval, perfect reconstruction, mask evenness,
     sharpness figures, plane-wave wedge predictions, wedge-centre share).
 

@@ -297,13 +297,30 @@ def group_items(T):
             yield j, i, lv, items
 
 
+# Threads of the float64 FFTs (scipy.fft's pocketfft) for the large checks;
+# 1 keeps NumPy's FFT.
+_FFT_WORKERS = 1
+
+
+def set_fft_workers(n):
+    """Run the oracle's float64 FFTs on n host threads (large volumes)."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = max(1, int(n))
+
+
 def rfft3(x):
     """Unnormalized rfft halving axis 0 (Julia's first axis)."""
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sfft
+        return sfft.rfftn(x, axes=(1, 2, 0), workers=_FFT_WORKERS)
     return np.fft.rfftn(x, axes=(1, 2, 0))
 
 
 def irfft3(X, dims):
     """Normalized irfft restoring axis 0 of length dims[0]."""
+    if _FFT_WORKERS > 1:
+        import scipy.fft as sfft
+        return sfft.irfftn(X, s=(dims[1], dims[2], dims[0]), axes=(1, 2, 0), workers=_FFT_WORKERS)
     return np.fft.irfftn(X, s=(dims[1], dims[2], dims[0]), axes=(1, 2, 0))
 
 

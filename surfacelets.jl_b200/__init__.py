@@ -11,7 +11,7 @@ fallback: importing the package fails if the library is missing.
 from .autograd import analyze_ad, as_colmajor, synthesize_ad  # noqa: F401
 from .batch import Batch  # noqa: F401
 from .sharded import LibRanges, analyze_sharded, shard, synthesize_sharded  # noqa: F401
-from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateError, lib  # noqa: F401
+from ._lib import ArgumentError, CudaError, DimensionMismatch, LIB_PATH, StateError, DeviceWaitTimeout, lib  # noqa: F401
 from .transforms import (  # noqa: F401
     NDFB, HourglassFB, NSSurfacelet, Surfacelet, Workspace, adjoint_analyze, hourglass_decompose,
     hourglass_reconstruct, ndfb_decompose, ndfb_reconstruct, ndfb_subband_index, ndfb_subband_triple, adjoint_analyze_, adjoint_synthesize,

@@ -18,6 +18,7 @@ SFL_ERR_CUDA = -3
 SFL_ERR_ALLOC = -4
 SFL_ERR_STATE = -5
 SFL_ERR_UNSUPPORTED = -6
+SFL_ERR_TIMEOUT = -7
 SFL_MAX_SCALES = 16
 SFL_REAL32 = 0
 SFL_COMPLEX64 = 1
@@ -88,6 +89,7 @@ SIGNATURES = {
     "sfl_plan_tuning": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "sfl_plan_autotune": (C.c_int, [P, P, P, P]),
     "sfl_plan_status": (C.c_int, [P, C.POINTER(C.c_int32), C.c_int32]),
+    "sfl_plan_selftest_wait": (C.c_int, [P, P]),
     "sfl_analyze": (C.c_int, [P, P, P, P]),
     "sfl_synthesize": (C.c_int, [P, P, P, P]),
     "sfl_adjoint_analyze": (C.c_int, [P, P, P, P]),
@@ -141,6 +143,11 @@ class StateError(RuntimeError):
     pass
 
 
+class DeviceWaitTimeout(RuntimeError):
+    """A bounded device wait of an earlier call on the plan ran out; that
+    call's results are not valid (reported once by the next call)."""
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -170,4 +177,6 @@ def check(status):
         raise StateError(msg)
     if status == SFL_ERR_ALLOC:
         raise MemoryError(msg)
+    if status == SFL_ERR_TIMEOUT:
+        raise DeviceWaitTimeout(msg)
     raise CudaError(msg)

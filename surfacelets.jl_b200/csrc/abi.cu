@@ -32,6 +32,17 @@ DevMem::~DevMem() {
     if (p) cudaFree(p);
 }
 
+HostWord::~HostWord() {
+    if (host) cudaFreeHost(host);
+}
+
+void HostWord::alloc() {
+    if (host) return;
+    cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&host), sizeof(int), cudaHostAllocMapped), "cudaHostAlloc(status)");
+    *static_cast<volatile int*>(host) = 0;
+    cuda_check(cudaHostGetDevicePointer(reinterpret_cast<void**>(&dev), host, 0), "cudaHostGetDevicePointer(status)");
+}
+
 void DevMem::alloc(size_t n) {
     if (p) {
         cudaFree(p);
@@ -71,6 +82,9 @@ int guarded(F&& f) {
     } catch (const sfl::StateError& e) {
         g_error = e.what();
         return SFL_ERR_STATE;
+    } catch (const sfl::TimeoutError& e) {
+        g_error = e.what();
+        return SFL_ERR_TIMEOUT;
     } catch (const std::bad_alloc&) {
         g_error = "host memory exhausted";
         return SFL_ERR_ALLOC;
@@ -116,6 +130,20 @@ void on_device(const sfl_plan* plan, F&& f) {
         throw;
     }
     if (cur != plan->impl.device) sfl::cuda_check(cudaSetDevice(cur), "cudaSetDevice");
+}
+
+// A bounded wait of an earlier call on this plan ran out: report it once (the
+// word is cleared) before anything new is enqueued.  Results of the earlier
+// call are not valid.
+void check_timeout(const sfl_plan* plan) {
+    if (plan->impl.kind != SFL_KIND_NS) return;
+    sfl::NSPlan& N = *plan->impl.ns;
+    const int v = N.status.read();
+    if (v != 0) {
+        N.status.clear();
+        throw sfl::TimeoutError("a bounded device wait of an earlier call on this plan ran out (status " +
+                                std::to_string(v) + "); that call's results are not valid");
+    }
 }
 
 // Pipeline and group of an NS plan (the two knobs of the tuner).
@@ -488,13 +516,12 @@ int sfl_plan_status(sfl_plan* plan, int32_t* status, int32_t reset) {
         need(plan, "plan");
         need(status, "status");
         *status = 0;
-        if (plan->impl.kind == SFL_KIND_NS && plan->impl.ns->status.p) {
+        if (plan->impl.kind == SFL_KIND_NS) {
             on_device(plan, [&] {
-                int v = 0;
-                sfl::cuda_check(cudaMemcpy(&v, plan->impl.ns->status.p, sizeof(int), cudaMemcpyDeviceToHost),
-                                "cudaMemcpy(status)");
-                *status = v;
-                if (reset) sfl::cuda_check(cudaMemset(plan->impl.ns->status.p, 0, sizeof(int)), "cudaMemset(status)");
+                // the word is host memory the kernels store to: wait for the device's work first
+                sfl::cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+                *status = plan->impl.ns->status.read();
+                if (reset) plan->impl.ns->status.clear();
             });
         }
         return SFL_OK;
@@ -600,6 +627,7 @@ int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream) {
 int sfl_analyze(sfl_plan* plan, const void* x, void* c, void* stream) {
     return guarded([&] {
         need(plan, "plan");
+        check_timeout(plan);
         need(x, "x");
         need(c, "c");
         check_aligned(x, plan->impl.dtype, "x");
@@ -617,6 +645,7 @@ int sfl_analyze(sfl_plan* plan, const void* x, void* c, void* stream) {
 int sfl_synthesize(sfl_plan* plan, const void* c, void* x, void* stream) {
     return guarded([&] {
         need(plan, "plan");
+        check_timeout(plan);
         need(x, "x");
         need(c, "c");
         check_aligned(x, plan->impl.dtype, "x");
@@ -634,6 +663,7 @@ int sfl_synthesize(sfl_plan* plan, const void* c, void* x, void* stream) {
 int sfl_adjoint_analyze(sfl_plan* plan, const void* c, void* x, void* stream) {
     return guarded([&] {
         need(plan, "plan");
+        check_timeout(plan);
         need(x, "x");
         need(c, "c");
         check_aligned(x, plan->impl.dtype, "x");
@@ -651,6 +681,7 @@ int sfl_adjoint_analyze(sfl_plan* plan, const void* c, void* x, void* stream) {
 int sfl_adjoint_synthesize(sfl_plan* plan, const void* x, void* c, void* stream) {
     return guarded([&] {
         need(plan, "plan");
+        check_timeout(plan);
         need(x, "x");
         need(c, "c");
         check_aligned(x, plan->impl.dtype, "x");
@@ -672,9 +703,18 @@ static sfl::NSPlan& ns_of(sfl_plan* plan, const char* what = "streaming") {
     return *plan->impl.ns;
 }
 
+int sfl_plan_selftest_wait(sfl_plan* plan, void* stream) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan, "the bounded-wait self-test");
+        on_device(plan, [&] { sfl::ns_selftest_wait(N, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
 int sfl_stream_analyze_begin(sfl_plan* plan, const void* x, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = ns_of(plan);
+        check_timeout(plan);
         need(x, "x");
         on_device(plan, [&] { sfl::ns_stream_analyze_begin(N, x, as_stream(stream)); });
         return SFL_OK;
@@ -684,6 +724,7 @@ int sfl_stream_analyze_begin(sfl_plan* plan, const void* x, void* stream) {
 int sfl_stream_analyze_next(sfl_plan* plan, void* band, int32_t* index, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = ns_of(plan);
+        check_timeout(plan);
         need(band, "band");
         need(index, "index");
         int r = SFL_OK, idx = 0;
@@ -696,6 +737,7 @@ int sfl_stream_analyze_next(sfl_plan* plan, void* band, int32_t* index, void* st
 int sfl_stream_synthesize_begin(sfl_plan* plan, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = ns_of(plan);
+        check_timeout(plan);
         sfl::ns_stream_synth_begin(N, as_stream(stream));
         return SFL_OK;
     });
@@ -715,6 +757,7 @@ int sfl_stream_synthesize_next_index(sfl_plan* plan, int32_t* index) {
 int sfl_stream_synthesize_push(sfl_plan* plan, const void* band, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = ns_of(plan);
+        check_timeout(plan);
         need(band, "band");
         on_device(plan, [&] { sfl::ns_stream_synth_push(N, band, as_stream(stream)); });
         return SFL_OK;
@@ -724,6 +767,7 @@ int sfl_stream_synthesize_push(sfl_plan* plan, const void* band, void* stream) {
 int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = ns_of(plan);
+        check_timeout(plan);
         need(x, "x");
         on_device(plan, [&] { sfl::ns_stream_synth_end(N, x, as_stream(stream)); });
         return SFL_OK;
@@ -864,6 +908,7 @@ int sfl_ns_analyze_bf16(sfl_plan* plan, const void* x, void* c, float* scales, v
         need(c, "c");
         need(scales, "scales");
         sfl::NSPlan& N = ns_of(plan, "bfloat16 coefficients");
+        check_timeout(plan);
         if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
         check_aligned(x, plan->impl.dtype, "x");
         if (reinterpret_cast<uintptr_t>(c) % 2 != 0) throw sfl::ArgError("c is not aligned to its element type");
@@ -878,6 +923,7 @@ int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, v
         need(c, "c");
         need(scales, "scales");
         sfl::NSPlan& N = ns_of(plan, "bfloat16 coefficients");
+        check_timeout(plan);
         if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
         check_aligned(x, plan->impl.dtype, "x");
         if (reinterpret_cast<uintptr_t>(c) % 2 != 0) throw sfl::ArgError("c is not aligned to its element type");
@@ -892,6 +938,7 @@ int sfl_ns_denoise(sfl_plan* plan, const void* x, void* y, const float* tau, voi
         need(y, "y");
         need(tau, "tau");
         sfl::NSPlan& N = ns_of(plan, "the denoiser");
+        check_timeout(plan);
         if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
         check_aligned(x, plan->impl.dtype, "x");
         check_aligned(y, plan->impl.dtype, "y");
@@ -941,6 +988,7 @@ int sfl_ns_stream_order(const sfl_plan* plan, int32_t* subband_index) {
 int sfl_ns_forward_spectrum(sfl_plan* plan, const void* x, void* X, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = range_plan(plan);
+        check_timeout(plan);
         need(x, "x");
         need(X, "X");
         check_spectrum_aligned(X, "X");
@@ -958,6 +1006,7 @@ int sfl_ns_forward_spectrum(sfl_plan* plan, const void* x, void* X, void* stream
 int sfl_ns_analyze_range(sfl_plan* plan, const void* X, int32_t first, int32_t count, void* c, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = range_plan(plan);
+        check_timeout(plan);
         need(X, "X");
         check_spectrum_aligned(X, "X");
         need(c, "c");
@@ -983,6 +1032,7 @@ int sfl_ns_accumulate_range(sfl_plan* plan, const void* c, int32_t first, int32_
                             void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = range_plan(plan);
+        check_timeout(plan);
         need(c, "c");
         need(A, "A");
         check_spectrum_aligned(A, "A");
@@ -992,7 +1042,7 @@ int sfl_ns_accumulate_range(sfl_plan* plan, const void* c, int32_t first, int32_
         on_device(plan, [&] {
             for (int ch = 0; ch < N.nch; ++ch) {
                 float2* acc = static_cast<float2*>(A) + ch * E;
-                float2* comp = N.comp.as<float2>() + (N.slab ? 0 : ch * N.H);
+                float2* comp = sfl::ns_comp_grid(N, ch);
                 if (clear) sfl::ns_acc_clear(N, acc, comp, as_stream(stream));
                 for (int i0 = first, i1; i0 < first + count; i0 = i1) {
                     i1 = std::min(sfl::ns_next_chunk(N, i0), first + count);
@@ -1010,6 +1060,7 @@ int sfl_ns_accumulate_range(sfl_plan* plan, const void* c, int32_t first, int32_
 int sfl_ns_inverse_spectrum(sfl_plan* plan, void* A, void* x, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = range_plan(plan);
+        check_timeout(plan);
         need(A, "A");
         check_spectrum_aligned(A, "A");
         need(x, "x");

@@ -29,6 +29,15 @@ __device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2
 __device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+// Kahan step s += v with compensation c (Kahan 1965), per component:
+// y = v - c; t = s + y; c = (t - s) - y; s = t.  The explicit round-to-nearest
+// intrinsics keep the compiler from contracting or reordering it.
+__device__ __forceinline__ void kahan_add(float2& s, float2& c, float2 v) {
+    const float yx = __fsub_rn(v.x, c.x), yy = __fsub_rn(v.y, c.y);
+    const float tx = __fadd_rn(s.x, yx), ty = __fadd_rn(s.y, yy);
+    c = make_float2(__fsub_rn(__fsub_rn(tx, s.x), yx), __fsub_rn(__fsub_rn(ty, s.y), yy));
+    s = make_float2(tx, ty);
+}
 // multiply by -i (forward) or +i (inverse)
 __device__ __forceinline__ float2 c_rot(float2 a, bool inv) {
     return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);

@@ -21,6 +21,7 @@
 #include "passes.cuh"
 #include "plan.h"
 #include "regpass.cuh"
+#include "tma.cuh"
 
 namespace sfl {
 
@@ -393,8 +394,7 @@ void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtyp
     get_fft(P.ffts, dims[1]);
     get_fft(P.ffts, dims[2]);
 
-    P.status.alloc(sizeof(int));
-    cuda_check(cudaMemset(P.status.p, 0, sizeof(int)), "cudaMemset(status)");
+    P.status.alloc();
     P.group = std::min(8, P.S);
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
@@ -413,7 +413,7 @@ void ns_alloc_scratch(NSPlan& P) {
     P.work.alloc(sizeof(float2) * spec * P.group * (P.slab ? P.nch : 1));
     if (P.slab) {
         P.acc.alloc(sizeof(float2) * spec * P.nch);
-        P.comp.alloc(0);
+        P.comp.alloc(sizeof(float2) * spec * P.nch);
     } else {
         P.acc.alloc(sizeof(float2) * P.H * std::max(P.nch, P.group * P.nch));
         P.comp.alloc(sizeof(float2) * P.H * P.nch);
@@ -672,13 +672,15 @@ void ns_analyze_range(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, i
 
 void ns_acc_clear(NSPlan& P, float2* acc, float2* comp, cudaStream_t st) {
     cuda_check(cudaMemsetAsync(acc, 0, sizeof(float2) * ns_spec_elems(P), st), "cudaMemsetAsync(acc)");
-    if (!P.slab) cuda_check(cudaMemsetAsync(comp, 0, sizeof(float2) * P.H, st), "cudaMemsetAsync(comp)");
+    cuda_check(cudaMemsetAsync(comp, 0, sizeof(float2) * ns_spec_elems(P), st), "cudaMemsetAsync(comp)");
 }
+
+float2* ns_comp_grid(NSPlan& P, int ch) { return P.comp.as<float2>() + ch * ns_spec_elems(P); }
 
 void ns_accumulate_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
                          float2* acc, float2* comp, cudaStream_t st) {
     if (P.slab)
-        ns_slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, st);
+        ns_slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, comp, st);
     else
         synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, comp, false, st);
 }
@@ -697,7 +699,7 @@ void ns_stage_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz
 void ns_accum_staged(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, int nch,
                      cudaStream_t st) {
     if (P.slab) {
-        ns_slab_accum_items(P, i0, nz, analysis_masks, acc, nch, st);
+        ns_slab_accum_items(P, i0, nz, analysis_masks, acc, comp, nch, st);
     } else {
         if (nch != 1) throw ArgError("the line pipeline stages one channel at a time");
         accum_items(P, i0, nz, analysis_masks, acc, comp, false, st);
@@ -795,6 +797,25 @@ void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool anal
     }
 }
 
+// ── bounded-wait self-test ──────────────────────────────────────────────────
+
+// One CTA waits, with a short iteration limit, on an mbarrier that expects
+// one arrival nobody makes (no copy is issued): the wait runs out and records
+// its status through the same path as the bulk-copy waits.
+__global__ void selftest_wait_kernel(int* status, long long limit) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+        mbar_wait_bounded(&bar, 0, status, limit);
+    }
+}
+
+void ns_selftest_wait(NSPlan& P, cudaStream_t st) {
+    selftest_wait_kernel<<<1, 32, 0, st>>>(P.status.dev, 4096);
+    cuda_check(cudaGetLastError(), "selftest_wait_kernel launch");
+}
+
 // ── streaming ────────────────────────────────────────────────────────────────
 
 void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
@@ -848,7 +869,7 @@ void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
     } else {
         const long long E = ns_spec_elems(P);
         if (P.stream_pos == 0) {
-            for (int ch = 0; ch < P.nch; ++ch) ns_acc_clear(P, P.acc.as<float2>() + ch * E, P.comp.as<float2>() + ch * P.H, st);
+            for (int ch = 0; ch < P.nch; ++ch) ns_acc_clear(P, P.acc.as<float2>() + ch * E, ns_comp_grid(P, ch), st);
             P.stream_chunk0 = 0;
         }
         if (P.slab || P.nch == 1) {
@@ -865,7 +886,7 @@ void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
             // complex data on the line pipeline: the work slots hold one channel
             for (int ch = 0; ch < P.nch; ++ch)
                 ns_accumulate_range(P, reinterpret_cast<const float*>(band) + ch, ZMap{}, P.nch, P.stream_pos, 1,
-                                    false, P.acc.as<float2>() + ch * E, P.comp.as<float2>() + ch * P.H, st);
+                                    false, P.acc.as<float2>() + ch * E, ns_comp_grid(P, ch), st);
         }
     }
     P.stream_pos += 1;

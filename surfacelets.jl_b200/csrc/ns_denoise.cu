@@ -46,7 +46,7 @@ void ns_denoise(NSPlan& P, const float* x, float* y, const float* tau, cudaStrea
         i1 = ns_next_chunk(P, i0);
         const int nz = i1 - i0;
         if (P.slab) {
-            ns_slab_denoise_items(P, X, i0, nz, tau, A, st);
+            ns_slab_denoise_items(P, X, i0, nz, tau, A, K, st);
             continue;
         }
         if (fused_lines) {

@@ -574,7 +574,7 @@ PlaneArgs plane_args(NSPlan& P) {
     a.n3 = P.dims[2];
     a.E = (long long)P.dims[1] * P.dims[2];
     a.H = P.H;
-    a.status = P.status.as<int>();
+    a.status = P.status.dev;
     return a;
 }
 

@@ -129,9 +129,14 @@ constexpr int accum_minb() { return (N == 96 || N == 160 || N >= 256) ? 1 : 2; }
 // Accumulation lengths whose sums go to shared memory (their register form spills).
 template <int N>
 constexpr bool accum_sums_shared() { return N == 96 || N == 128 || N == 160; }
+// Lengths whose Kahan compensations go to shared memory beside the sums (160: the exchange rows and the
+// sums leave no room, so its compensations stay in registers).
+template <int N>
+constexpr bool accum_comps_shared() { return N == 96 || N == 128; }
 template <int N>
 constexpr size_t accum_smem() {
-    return RegGeom<N>::SMEM + (accum_sums_shared<N>() ? sizeof(float2) * RegGeom<N>::M * RegGeom<N>::N2 * 256 : 0);
+    constexpr size_t plane = sizeof(float2) * RegGeom<N>::M * RegGeom<N>::N2 * 256;
+    return RegGeom<N>::SMEM + (accum_sums_shared<N>() ? plane : 0) + (accum_comps_shared<N>() ? plane : 0);
 }
 
 // Analysis line pass over IPC subbands of one mask group per CTA: a line's X
@@ -210,18 +215,24 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
 }
 
 // Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
-// summed in registers into the accumulator (plain float32 sums, item order).
+// added into the accumulator with Kahan compensation (item order).  The
+// running sums and their compensations are loaded from acc / comp, carried in
+// registers or shared memory across the group's items, and stored back: one
+// round trip of both per group, so the compensation spans the whole synthesis
+// (src/transforms/ns_surfacelet.jl:292, 355, 383 accumulate every subband
+// into one spectrum).
 template <int N>
 __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(const float2* __restrict__ Y, long long ystride, int G,
                                                             int P1, int s3, BoxMap bx, NSMaskTables tb,
                                                             const NSItem* __restrict__ items, int item0, int synth,
-                                                            float2* acc, const float2* __restrict__ tw, int nlines,
-                                                            long long ychs, long long achs) {
+                                                            float2* acc, float2* comp, const float2* __restrict__ tw,
+                                                            int nlines, long long ychs, long long achs) {
     using Ge = RegGeom<N>;
     constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
     extern __shared__ float2 xch[];
     Y += blockIdx.y * ychs;   // channel
     acc += blockIdx.y * achs;
+    comp += blockIdx.y * achs;
     const int tid = threadIdx.x;
     const int lp = tid % LP, p = tid / LP;
     const int l = blockIdx.x * LP + lp;
@@ -229,23 +240,37 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
     int k1 = 0, k2 = 0;
     if (valid) bx.k12(l, k1, k2);
     float2* a = acc + k1 + P1 * k2;
+    float2* ca = comp + k1 + P1 * k2;
     float2* xl = xch + lp * Ge::XLINE;
-    // the line's sums: in registers, or (lengths whose registers would spill) in shared memory after
-    // the exchange rows, value q of thread t at [q * 256 + t]
+    // the line's sums and compensations: in registers, or (lengths whose registers would spill) in shared
+    // memory after the exchange rows, value q of thread t at [q * 256 + t] (sums), then the same for the
+    // compensations
     constexpr bool kSumsShared = accum_sums_shared<N>();
+    constexpr bool kCompsShared = accum_comps_shared<N>();
     float2 sr[kSumsShared ? 1 : E];
+    float2 cr[kCompsShared ? 1 : E];
     float2* ss = xch + LP * Ge::XLINE + tid;
+    float2* cs = ss + (kSumsShared ? E * Ge::THREADS : 0);
     auto sum = [&](int q) -> float2& {
         if constexpr (kSumsShared)
             return ss[q * Ge::THREADS];
         else
             return sr[q];
     };
+    auto cmp = [&](int q) -> float2& {
+        if constexpr (kCompsShared)
+            return cs[q * Ge::THREADS];
+        else
+            return cr[q];
+    };
 #pragma unroll
     for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
-        for (int k = 0; k < N2; ++k)
-            sum(j * N2 + k) = valid ? a[((p + N2 * j) + N1 * k) * s3] : make_float2(0.f, 0.f);
+        for (int k = 0; k < N2; ++k) {
+            const long long o = (long long)((p + N2 * j) + N1 * k) * s3;
+            sum(j * N2 + k) = valid ? a[o] : make_float2(0.f, 0.f);
+            cmp(j * N2 + k) = valid ? ca[o] : make_float2(0.f, 0.f);
+        }
     const long long si_nat = (long long)tb.h1 * tb.n2;
     const int lnat = k1 + tb.h1 * k2;
     // the group factor of the line (group table, bandpass table or the lowpass factors), once for all items
@@ -273,8 +298,7 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
             for (int k = 0; k < N2; ++k) {
                 const int k3 = (p + N2 * j) + N1 * k;
                 const float m = wedges ? gf[j * N2 + k] * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]) : gf[j * N2 + k];
-                float2& t = sum(j * N2 + k);
-                t = c_add(t, c_scale(u[j * N2 + k], m));
+                kahan_add(sum(j * N2 + k), cmp(j * N2 + k), c_scale(u[j * N2 + k], m));
             }
         __syncthreads();   // the exchange rows are reused by the next item
     }
@@ -282,7 +306,11 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
 #pragma unroll
         for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
-            for (int k = 0; k < N2; ++k) a[((p + N2 * j) + N1 * k) * s3] = sum(j * N2 + k);
+            for (int k = 0; k < N2; ++k) {
+                const long long o = (long long)((p + N2 * j) + N1 * k) * s3;
+                a[o] = sum(j * N2 + k);
+                ca[o] = cmp(j * N2 + k);
+            }
     }
 }
 
@@ -811,7 +839,7 @@ SlabArgs slab_args(const NSPlan& P, const NSBox& b, int nz) {
     a.twb = P.ffts.at(P.dims[1])->sh.tw;
     a.es = 1;
     a.scale = 1.f;
-    a.status = P.status.as<int>();
+    a.status = P.status.dev;
     return a;
 }
 
@@ -824,7 +852,7 @@ void line3(const NSPlan& P, const Load& ld, const Store& so, int nlines, int nz,
 
 template <int N>
 void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& bx, int i0, int synth, float2* acc,
-                       int nlines, int nch, long long ychs, long long achs, cudaStream_t st) {
+                       float2* comp, int nlines, int nch, long long ychs, long long achs, cudaStream_t st) {
     using Ge = RegGeom<N>;
     static bool configured = false;
     if (!configured) {
@@ -836,7 +864,7 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
     dim3 grid((nlines + Ge::LP - 1) / Ge::LP, nch);
     int tok = prof_begin("ns_slab_accum_axis3", st);
     ns_slab_accum_kernel<N><<<grid, Ge::THREADS, accum_smem<N>(), st>>>(Y, P.SP, nz, P.P1, P.P1 * P.dims[1], bx, P.tb,
-                                                                 P.items.as<NSItem>(), i0, synth, acc,
+                                                                 P.items.as<NSItem>(), i0, synth, acc, comp,
                                                                  P.ffts.at(P.dims[2])->sh.tw, nlines, ychs, achs);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
@@ -954,23 +982,26 @@ void slab_mask_pass(NSPlan& P, const float2* X, int i0, int nz, bool synth_masks
     throw ArgError("no register line pass for axis 3 of this size");
 }
 
-// The synthesis axis-3 pass of items [i0, i0 + nz) from Y into acc + ch SP.
-void slab_accum_pass(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, int nch, cudaStream_t st) {
+// The synthesis axis-3 pass of items [i0, i0 + nz) from Y into acc + ch SP,
+// Kahan-compensated through comp + ch SP.
+void slab_accum_pass(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, int nch,
+                     cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     const float2* Y = P.work.as<float2>();
-    prof_bytes("ns_slab_accum_axis3", nch * (nz * box_bytes(P, b) + 0.5 * box_bytes(P, b) + 2 * box_bytes(P, b)));
+    // Y once per item, the group table (4 B a bin), the accumulator and its compensation in and out
+    prof_bytes("ns_slab_accum_axis3", nch * (nz * box_bytes(P, b) + 0.5 * box_bytes(P, b) + 4 * box_bytes(P, b)));
     const BoxMap bx = box_map(P, b);
     const int nl = b.nk1 * b.nk2;
     const int sy = analysis_masks ? 0 : 1;
     const long long yc = ych_stride(P), ac = P.SP;
     switch (P.dims[2]) {
-        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
-        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
-        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
-        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
-        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
-        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
-        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, nl, nch, yc, ac, st); return;
+        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
     }
     throw ArgError("no register line pass for axis 3 of this size");
 }
@@ -1014,15 +1045,15 @@ void slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int 
 // Synthesis accumulation of items [i0, i0 + nz) (one mask group) read from
 // vol + vz.off(z) (+ ch) into acc + ch SP.
 void slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
-                      float2* acc, int nch, cudaStream_t st) {
+                      float2* acc, float2* comp, int nch, cudaStream_t st) {
     slab_stage_items(P, vol, vz, es, i0, nz, 0, nch, st);
-    slab_accum_pass(P, i0, nz, analysis_masks, acc, nch, st);
+    slab_accum_pass(P, i0, nz, analysis_masks, acc, comp, nch, st);
 }
 
 // The denoiser on items [i0, i0 + nz) (one mask group; real data): the
 // analysis axis-3 pass into Y, the shrink slab pass in place, the synthesis
 // accumulation.
-void slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
+void slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc, float2* comp,
                         cudaStream_t st) {
     const NSBox& b = item_box(P, i0);
     slab_mask_pass(P, X, i0, nz, false, 1, st);
@@ -1035,7 +1066,7 @@ void slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float*
     a.items = P.items.as<NSItem>();
     a.item0 = i0;
     launch_slab<2>(P.dims[0], P.dims[1], a, P.sms, slab_smem(P.dims[0], P.dims[1]), st, "ns_slab_shrink");
-    slab_accum_pass(P, i0, nz, false, acc, 1, st);
+    slab_accum_pass(P, i0, nz, false, acc, comp, 1, st);
 }
 
 // Consecutive items of one mask group, at most P.group of them.
@@ -1112,11 +1143,13 @@ void ns_slab_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool sy
 void ns_slab_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
     const int nch = P.nch;
     float2* A = P.acc.as<float2>();
+    float2* K = P.comp.as<float2>();
     cuda_check(cudaMemsetAsync(A, 0, sizeof(float2) * P.SP * nch, st), "cudaMemsetAsync(acc)");
+    cuda_check(cudaMemsetAsync(K, 0, sizeof(float2) * P.SP * nch, st), "cudaMemsetAsync(comp)");
     for (int i0 = 0, i1; i0 < P.S; i0 = i1) {
         i1 = chunk_end(P, i0);
         slab_synth_items(P, static_cast<const float*>(c), ns_subband_map(P, i0, nch), nch, i0, i1 - i0,
-                         analysis_masks, A, nch, st);
+                         analysis_masks, A, K, nch, st);
     }
     slab_irfft3(P, A, static_cast<float*>(x), nch, nch, st);
 }
@@ -1129,13 +1162,13 @@ void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int 
 }
 
 void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
-                         float2* acc, cudaStream_t st) {
-    slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, 1, st);
+                         float2* acc, float2* comp, cudaStream_t st) {
+    slab_synth_items(P, vol, vz, es, i0, nz, analysis_masks, acc, comp, 1, st);
 }
 
-void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
+void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc, float2* comp,
                            cudaStream_t st) {
-    slab_denoise_items(P, X, i0, nz, tau, acc, st);
+    slab_denoise_items(P, X, i0, nz, tau, acc, comp, st);
 }
 
 void ns_slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
@@ -1143,8 +1176,9 @@ void ns_slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, i
     slab_stage_items(P, vol, vz, es, i0, nz, slot0, nch, st);
 }
 
-void ns_slab_accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, int nch, cudaStream_t st) {
-    slab_accum_pass(P, i0, nz, analysis_masks, acc, nch, st);
+void ns_slab_accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, int nch,
+                         cudaStream_t st) {
+    slab_accum_pass(P, i0, nz, analysis_masks, acc, comp, nch, st);
 }
 
 }  // namespace sfl

@@ -22,10 +22,30 @@ struct AllocError : std::runtime_error {
 struct StateError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
+// A bounded device wait of an earlier call ran out (the plan's status word).
+struct TimeoutError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
 
 void cuda_check(cudaError_t e, const char* what);
 
 // Device allocation owned by a plan.
+// One int in mapped, page-locked host memory: kernels store to it through
+// `dev`, the host reads `host` without a copy or a synchronisation.
+struct HostWord {
+    int* host = nullptr;
+    int* dev = nullptr;
+    HostWord() = default;
+    HostWord(const HostWord&) = delete;
+    HostWord& operator=(const HostWord&) = delete;
+    ~HostWord();
+    void alloc();
+    int read() const { return host ? *static_cast<volatile int*>(host) : 0; }
+    void clear() {
+        if (host) *static_cast<volatile int*>(host) = 0;
+    }
+};
+
 struct DevMem {
     void* p = nullptr;
     size_t bytes = 0;
@@ -115,7 +135,7 @@ struct NSPlan {
     bool plane = false;
     DevMem Gp, Blp;         // G and Bl in plane-major order
     NSMaskTables tbp;
-    DevMem status;          // device status word of bounded waits (0 = fine)
+    HostWord status;        // status word of bounded waits (0 = fine), written by the kernels
     // slab pipeline (spectra with the axis-1 pitch padded to P1)
     bool slab = false;
     int P1 = 0;
@@ -182,12 +202,13 @@ int ns_slab_chunk_end(const NSPlan& P, int i0);
 void ns_slab_analyze_items(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
                            cudaStream_t st);
 void ns_slab_synth_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
-                         float2* acc, cudaStream_t st);
-void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc,
+                         float2* acc, float2* comp, cudaStream_t st);
+void ns_slab_denoise_items(NSPlan& P, const float2* X, int i0, int nz, const float* tau, float2* acc, float2* comp,
                            cudaStream_t st);
 void ns_slab_stage_items(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, int slot0, int nch,
                          cudaStream_t st);
-void ns_slab_accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, int nch, cudaStream_t st);
+void ns_slab_accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, float2* comp, int nch,
+                         cudaStream_t st);
 // The line pipeline's denoiser step on items [i0, i0 + nz): the analysis
 // axis-3 and axis-2 passes, one fused axis-1 kernel (C2R, soft threshold,
 // R2C), the synthesis axis-2 pass and the accumulation (ns.cu); for axis-1
@@ -207,6 +228,11 @@ int ns_next_chunk(const NSPlan& P, int i0);
 void ns_analyze_range(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
                       cudaStream_t st);
 void ns_acc_clear(NSPlan& P, float2* acc, float2* comp, cudaStream_t st);
+// The plan's Kahan compensation grid of channel ch (spectrum-sized).
+float2* ns_comp_grid(NSPlan& P, int ch);
+// Runs out one bounded mbarrier wait on purpose (no copy in flight) so that
+// the plan's status word records a timeout.
+void ns_selftest_wait(NSPlan& P, cudaStream_t st);
 void ns_accumulate_range(NSPlan& P, const float* vol, ZMap vz, int es, int i0, int nz, bool analysis_masks,
                          float2* acc, float2* comp, cudaStream_t st);
 void ns_inverse_spectrum(NSPlan& P, float2* A, float* x, int es, cudaStream_t st);

@@ -1,8 +1,8 @@
 // Bulk asynchronous copies (TMA, cp.async.bulk) between global and shared
 // memory, completed on an mbarrier, for sm_100a.  Every wait is bounded: a
 // wait that runs out of iterations records an error code in the plan's
-// device status word (read by the host through sfl_plan_status) and gives up
-// instead of spinning forever.
+// status word (mapped host memory, read through sfl_plan_status and checked
+// by the next call on the plan) and gives up instead of spinning forever.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -43,11 +43,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
 }
 
 // Waits for `phase` of the barrier with an iteration limit; false on timeout
-// (*status then holds kStatusMbarTimeout).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, int* status) {
-    for (long long it = 0; it < kMbarSpinLimit; ++it)
+// (*status then holds kStatusMbarTimeout).  The status word is mapped host
+// memory: a plain store, made visible to the host by a system-scope fence.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, int* status,
+                                                  long long limit = kMbarSpinLimit) {
+    for (long long it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, phase)) return true;
-    atomicExch(status, kStatusMbarTimeout);
+    *reinterpret_cast<volatile int*>(status) = kStatusMbarTimeout;
+    __threadfence_system();
     return false;
 }
 
