@@ -258,15 +258,20 @@ int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream);
  * `index` (1-based, subband_layout order) of the real float32 volume x to
  * `band` (device memory of the plan's dims), and allocates nothing: its
  * scratch is a static 4 MiB device array inside the library, so it suits
- * callers that cannot allocate device memory when they transform (host
- * functions enqueued on a stream, allocation-free real-time loops, processes
- * whose memory manager owns the device).  Create the plan (which allocates
- * the mask tables) beforehand.  Limits: real plans only, and
- * (n1/2+1)*n2*n3 <= 262144 (e.g. 64^3); larger sizes return SFL_ERR_ARGUMENT.
- * The first call on a device looks up the scratch's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the scratch: calls that overlap on the GPU race, so order
- * them (one stream, or explicit synchronization). */
+ * callers that cannot allocate device memory when they transform
+ * (allocation-free real-time loops, processes whose memory manager owns the
+ * device).  Call it from ordinary host code: it launches kernels, so it may
+ * not run inside a cudaLaunchHostFunc callback.  Create the plan (which
+ * allocates the mask tables) beforehand, and make the first call for each
+ * plan size at start-up too: the first call on a device looks up the
+ * scratch's device address (cudaGetSymbolAddress), and under lazy module
+ * loading a kernel's first launch loads its code; both belong before the
+ * allocation-free phase and before any stream capture.  The address is
+ * cached per device for the process; do not call this again on a device
+ * after cudaDeviceReset.  Limits: real plans only, and (n1/2+1)*n2*n3 <=
+ * 262144 (e.g. 64^3); larger sizes return SFL_ERR_ARGUMENT.  All calls share
+ * the scratch: calls that overlap on the GPU race, so order them (one
+ * stream, or explicit synchronization). */
 int sfl_ns_analyze_subband_static(sfl_plan* plan, const void* x, void* band, int32_t index, void* stream);
 
 /* ── Design tables (host only; for tests and inspection) ──────────────────

@@ -776,7 +776,7 @@ int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream) {
 
 int sfl_ns_analyze_subband_static(sfl_plan* plan, const void* x, void* band, int32_t index, void* stream) {
     return guarded([&] {
-        sfl::NSPlan& N = ns_of(plan);
+        sfl::NSPlan& N = ns_of(plan, "sfl_ns_analyze_subband_static");
         need(x, "x");
         need(band, "band");
         check_aligned(x, plan->impl.dtype, "x");

@@ -2,14 +2,25 @@
 // static device array of this library instead of memory it allocates.
 //
 // Who needs it: callers that must not allocate device memory at the moment
-// they transform — code running in a host function enqueued on a CUDA stream
-// (the CUDA runtime forbids runtime API calls such as cudaMalloc there),
-// latency-critical loops that cannot absorb an allocator call, and
+// they transform — latency-critical loops that cannot absorb an allocator
+// call (or the device-wide synchronisation a cudaFree implies), and
 // applications whose own memory manager owns the whole device and forbids
 // side allocations.  Such a caller creates the plan once at start-up (that
-// step allocates the mask tables) and then calls
-// sfl_ns_analyze_subband_static as often as it likes: the call itself
-// allocates nothing, neither through cudaMalloc nor through any library.
+// step allocates the mask tables), makes one warm-up call per plan size
+// there too, and then calls sfl_ns_analyze_subband_static as often as it
+// likes from ordinary host code: the call itself allocates nothing, neither
+// through cudaMalloc nor through any library.  It does launch kernels, so it
+// cannot run inside a host function enqueued on a stream (cudaLaunchHostFunc
+// callbacks may make no CUDA call at all).
+//
+// Warm-up: the first call on a device looks up the scratch's device address
+// (cudaGetSymbolAddress), and under CUDA's lazy module loading the first
+// launch of a kernel loads its code, which can take device memory; so the
+// first call for each plan size belongs at start-up, before the
+// allocation-free phase and before any stream capture.  The cached address
+// is per device and per process: after cudaDeviceReset the library's module
+// is loaded anew and the cache is stale, so a process that resets a device
+// must not call this entry point on it again.
 //
 // The scratch is g_static_scratch below, kNoAllocMaxPoints x 2 complex
 // float32 values (4 MiB): the input spectrum and one work spectrum on the

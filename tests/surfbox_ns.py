@@ -44,16 +44,21 @@ def reference_weights(octant):
     return tight_dev, tuple(v[k][:17] ** 2 / 3.0 for k in range(3))
 
 
-def hourglass_statistics(w_mine, w_ref):
+def hourglass_statistics(w_mine, w_ref, tie_tol=0.0):
     """The geometric figures the reference asserts on
     (test/items/test_surfbox_reference.jl:44-74): the cross-distance matrix
     d[k][m] = max |W_k - W_ref_m|, the dominant-hourglass agreement, the
     median and maximum of the reference's top-two gap over the disagreeing
-    bins, the mean gap over all bins, and the mean |W - W_ref|."""
+    bins, the mean gap over all bins, and the mean |W - W_ref|.
+
+    The dominant hourglass is the first maximum, as Julia's argmax.  tie_tol
+    counts weights within tie_tol of the maximum as tied (first index wins):
+    float32 weights carry rounding noise of a few ulps, which would otherwise
+    decide the bins where the hourglasses meet with equal weight."""
     d = [[float(np.max(np.abs(w_mine[k] - w_ref[m]))) for m in range(3)] for k in range(3)]
     wm = np.stack([w.ravel() for w in w_mine])
     wr = np.stack([w.ravel() for w in w_ref])
-    dom_m = np.argmax(wm, axis=0)          # first maximum, as Julia's argmax
+    dom_m = np.argmax(wm >= wm.max(axis=0) - tie_tol, axis=0)
     dom_r = np.argmax(wr, axis=0)
     s = -np.sort(-wr, axis=0)
     gap = s[0] - s[1]

@@ -7,8 +7,10 @@ with M a seeded Bernoulli(0.25) sampling mask with a fully sampled 16^3 centre
 and y = M o FFT3(phantom):
 the device gradient is held against the float64 oracle gradient (itself
 pinned by central differences in test_oracle_gradients.py), and the same for
-the gradient through analyze, x -> L(analyze(x)).  At 128^3 the device
-gradient is checked by central differences of the device loss."""
+the gradient through analyze, x -> L(analyze(x)).  At 128^3 (the workload's
+size) the device gradient is held against the float64 oracle's gradient and
+the oracle's float64 central differences (h = 1e-4, 32 directions), and by
+central differences of the device loss."""
 
 import numpy as np
 import pytest
@@ -86,3 +88,65 @@ def test_device_gradient_by_central_differences_at_128(sfl):
         fd = (loss64(c.detach() + h * d) - loss64(c.detach() - h * d)) / (2 * h)
         an = float((grad.conj() * d).real.double().sum())
         assert abs(fd - an) <= 2e-3 * abs(an), (fd, an)
+
+
+def test_gradients_at_128_against_the_float64_oracle_and_its_central_differences(sfl):
+    """The complex workload as stated: ComplexF32 128^3, NSSurfacelet(3, [2, 2, 3]).
+    The device gradient in c, and through analyze, against the float64
+    oracle's gradient (the reference's CPU gradient: synthesis' adjoint is
+    analysis, test/items/test_ns_surfacelet.jl:218-237); and the oracle's
+    float64 central differences, h = 1e-4 along 32 random unit directions,
+    against both the oracle gradient and the device gradient.  Synthesis is
+    linear, so L(c +- h d) is evaluated from synthesize(c) +- h synthesize(d),
+    all in float64 (one oracle synthesis per direction)."""
+    import os
+
+    import scipy.fft as sfft
+    from cs_problem import synthesize_c
+    dims = (128, 128, 128)
+    kw = dict(scales=3, direction_levels=[2, 2, 3])
+    N.set_fft_workers(os.cpu_count() or 1)
+    try:
+        T = N.make_tables(N.NSParams.make(**kw), dims)
+        ph, M, y, rng = make_problem(dims, 4)
+        ws = sfl.make_workspace(sfl.NSSurfacelet(**kw), "complex64", dims)
+        Md = torch.from_numpy(M.astype(np.float32)).cuda()
+        yd = torch.from_numpy(y.astype(np.complex64)).cuda()
+        gen = torch.Generator(device="cuda").manual_seed(9)
+        c0 = sfl.analyze(ws, sfl.to_device(ph.astype(np.complex64)))
+        cd = sfl.as_colmajor(c0 + 0.1 * torch.randn(c0.shape, dtype=torch.complex64, generator=gen,
+                                                    device="cuda")).detach()
+        c = sfl.to_host(cd).astype(np.complex128)          # the same point, in float64
+        cd.requires_grad_(True)
+        device_loss(sfl, ws, cd, Md, yd).backward()
+        gd = sfl.to_host(sfl.as_colmajor(cd.grad)).astype(np.complex128)
+        g = oracle_grad(T, c, M, y)
+        assert np.linalg.norm(gd - g) / np.linalg.norm(g) <= 1e-5
+        # central differences of the float64 loss
+        x = synthesize_c(T, c)
+        reg = lambda cc: LAM * np.sum(np.sqrt(cc.real ** 2 + cc.imag ** 2 + EPS ** 2))
+        h = 1e-4
+        for k in range(32):
+            dd = torch.randn(c0.shape, dtype=torch.complex64, generator=gen, device="cuda")
+            d = sfl.to_host(sfl.as_colmajor(dd)).astype(np.complex128)
+            d /= np.linalg.norm(d)
+            sd = synthesize_c(T, d)
+            w = os.cpu_count() or 1
+            lp = 0.5 * np.sum(np.abs(M * sfft.fftn(x + h * sd, workers=w) - y) ** 2) + reg(c + h * d)
+            lm = 0.5 * np.sum(np.abs(M * sfft.fftn(x - h * sd, workers=w) - y) ** 2) + reg(c - h * d)
+            fd = (lp - lm) / (2 * h)
+            an = float(np.sum((np.conj(g) * d).real))
+            an_dev = float(np.sum((np.conj(gd) * d).real))
+            assert abs(fd - an) <= 1e-6 * abs(an) + 1e-9 * np.linalg.norm(g), (k, fd, an)
+            assert abs(fd - an_dev) <= 1e-4 * abs(an) + 1e-5 * np.linalg.norm(g) / np.sqrt(d.size), (k, fd, an_dev)
+        del cd, c0
+        # through analyze: x -> L(analyze(x)), away from the data
+        xa = (ph + 0.1 * (rng.standard_normal(dims) + 1j * rng.standard_normal(dims))).astype(np.complex64)
+        xd = sfl.to_device(xa).requires_grad_(True)
+        ca = sfl.analyze_ad(ws, xd)
+        device_loss(sfl, ws, ca, Md, yd).backward()
+        gx = analyze_t_c(T, oracle_grad(T, analyze_c(T, xa.astype(np.complex128)), M, y))
+        gxd = sfl.to_host(sfl.as_colmajor(xd.grad))
+        assert np.linalg.norm(gxd - gx) / np.linalg.norm(gx) <= 1e-4
+    finally:
+        N.set_fft_workers(1)

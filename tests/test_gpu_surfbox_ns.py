@@ -5,8 +5,10 @@ the C ABI in float32.
 The hourglass weights are read off the device transform itself: a unit impulse
 at the origin has a flat spectrum, so the subbands of hourglass_decompose are
 irfft(M_i) and their rfft gives back the analysis masks M_i = sqrt(W_i) to
-float32 rounding.  The reference's geometric bounds then apply as stated; the
-exact partition-of-unity bound (1e-12 in float64) becomes 1e-5.
+float32 rounding.  The reference's geometric bounds then apply as stated, with
+the dominant hourglass taken as the first of the weights within 1e-6 of the
+maximum (float32 noise would otherwise break the exact ties where hourglasses
+meet); the exact partition-of-unity bound (1e-12 in float64) becomes 1e-5.
 """
 
 import numpy as np
@@ -32,7 +34,8 @@ def test_device_hourglass_matches_surfbox_partition(sfl):
         assert np.max(np.abs(M.imag)) <= 1e-6          # real, even masks
     w_mine = tuple(M.real ** 2 for M in masks)
     assert np.max(np.abs(sum(w_mine) - 1.0)) <= 1e-5   # partition of unity, float32
-    SB.assert_hourglass_statistics(SB.hourglass_statistics(w_mine, w_ref))
+    # ties at 8 float32 ulps of 1 (the weights' rounding noise through the FFTs is ~1e-7)
+    SB.assert_hourglass_statistics(SB.hourglass_statistics(w_mine, w_ref, tie_tol=1e-6))
 
 
 def test_device_ndfb_matches_surfbox_wedge_partition(sfl):
