@@ -103,6 +103,15 @@ __device__ __forceinline__ NSMaskLine ns_mask_line(const NSMaskTables& tb, const
     return c;
 }
 
+// Plane a of a directional item at (k1, k2), for a plane constant along axis 3
+// (it.wa_hi != 2): the per-line scalar of NSMaskLine's wa[0], read with only
+// the plane's four fields.
+__device__ __forceinline__ float ns_wedge_a_line(const NSMaskTables& tb, const NSItem* it, int k1, int k2) {
+    const int off = it->wa_off, lo = it->wa_lo, hi = it->wa_hi, dlo = it->wa_dlo;
+    const int klo = lo == 0 ? k1 : k2, khi = hi == 0 ? k1 : k2;
+    return tb.planes[off + klo + dlo * khi];
+}
+
 __device__ __forceinline__ float ns_mask_at(const NSMaskLine& c, int k3, long long si) {
     if (c.low) return c.lowc * c.lowv[k3];
     float g = c.m[(long long)k3 * si];

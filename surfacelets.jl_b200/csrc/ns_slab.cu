@@ -140,15 +140,24 @@ constexpr size_t accum_smem() {
 }
 
 // Analysis line pass over IPC subbands of one mask group per CTA: a line's X
-// times the group factor is loaded once, then per subband scaled by its two
+// times the group factor is loaded once, then per subband scaled by its
 // wedge planes, transformed along axis 3 and stored.
+//
+// Wedge planes constant along axis 3 (plane a of hourglasses 1 and 2, over
+// (k1, k2)) are a per-line scalar and commute with the axis-3 FFT, so they
+// are applied after it: Y_s = wa_p(k1, k2) IFFT_3(X G wb_q).  With nbq > 0
+// the chunk is nbq plane-b wedges q times whole rows of plane-a wedges p
+// (item t = p nbq + q); the CTA takes the items q-major, and consecutive
+// items of one q share a single FFT.  Every such item uses this order of
+// operations whether or not it shares, so the values do not depend on the
+// chunking.
 template <int N, int IPC>
 __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel(const float2* __restrict__ X, int P1, int s3,
                                                                  BoxMap bx, NSMaskTables tb,
                                                                  const NSItem* __restrict__ items, int item0, int nz,
                                                                  int synth, float2* Y, long long ystride,
                                                                  const float2* __restrict__ tw, int nlines,
-                                                                 long long xchs, long long ychs) {
+                                                                 long long xchs, long long ychs, int nbq) {
     using Ge = RegGeom<N>;
     constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
     extern __shared__ float2 xch[];
@@ -163,9 +172,12 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
     float2* xl = xch + lp * Ge::XLINE;
     const long long si = (long long)tb.h1 * tb.n2;
     const int lnat = k1 + tb.h1 * k2;
-    const int z0 = blockIdx.y * IPC;
+    const int k0 = blockIdx.y * IPC;
+    const int rows = nbq > 0 ? nz / nbq : 0;
+    // chunk item of the k-th position (q-major when factored)
+    auto zof = [&](int k) { return nbq > 0 ? (k % rows) * nbq + k / rows : k; };
     // the group factor of the line (group table, bandpass table or the lowpass factors)
-    const NSMaskLine m0 = ns_mask_line(tb, items[item0 + z0], lnat, synth != 0);
+    const NSMaskLine m0 = ns_mask_line(tb, items[item0 + zof(k0)], lnat, synth != 0);
     const float2* xp = X + k1 + P1 * k2;
     float2 xg[N1];
 #pragma unroll
@@ -174,59 +186,72 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
         const float g = m0.low ? m0.lowc * m0.lowv[i] : m0.m[i * si];
         xg[r] = valid ? c_scale(xp[(long long)i * s3], g) : make_float2(0.f, 0.f);
     }
+    float2 u[E];
 #pragma unroll 1
     for (int zz = 0; zz < IPC; ++zz) {
-        const int z = z0 + zz;
-        if (z >= nz) break;   // uniform across the CTA
+        const int k = k0 + zz;
+        if (k >= nz) break;   // uniform across the CTA
+        const int z = zof(k);
         const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
         const bool wedges = !(mk.low || mk.plain);
-        // a wedge plane over (k1, k2) is constant along the line: one load (the same product, so the
-        // same float32 values as the per-element form)
-        float2 v[N1];
-        if (!wedges) {
+        // plane a constant along the line: applied after the FFT
+        const bool after = wedges && mk.was == 0;
+        const bool reuse = after && nbq > 0 && zz > 0 && (k - 1) / rows == k / rows;   // same q: uniform
+        if (!reuse) {
+            float2 v[N1];
+            if (!wedges) {
 #pragma unroll
-            for (int r = 0; r < N1; ++r) v[r] = xg[r];
-        } else if (mk.was == 0) {
-            const float a0 = mk.wa[0];
+                for (int r = 0; r < N1; ++r) v[r] = xg[r];
+            } else if (after) {
 #pragma unroll
-            for (int r = 0; r < N1; ++r) v[r] = c_scale(xg[r], a0 * mk.wb[(p + N2 * r) * mk.wbs]);
-        } else if (mk.wbs == 0) {
-            const float b0 = mk.wb[0];
+                for (int r = 0; r < N1; ++r) v[r] = c_scale(xg[r], mk.wb[(p + N2 * r) * mk.wbs]);
+            } else if (mk.wbs == 0) {
+                const float b0 = mk.wb[0];
 #pragma unroll
-            for (int r = 0; r < N1; ++r) v[r] = c_scale(xg[r], mk.wa[(p + N2 * r) * mk.was] * b0);
-        } else {
+                for (int r = 0; r < N1; ++r) v[r] = c_scale(xg[r], mk.wa[(p + N2 * r) * mk.was] * b0);
+            } else {
 #pragma unroll
-            for (int r = 0; r < N1; ++r) {
-                const int i = p + N2 * r;
-                v[r] = c_scale(xg[r], mk.wa[i * mk.was] * mk.wb[i * mk.wbs]);
+                for (int r = 0; r < N1; ++r) {
+                    const int i = p + N2 * r;
+                    v[r] = c_scale(xg[r], mk.wa[i * mk.was] * mk.wb[i * mk.wbs]);
+                }
             }
+            reg_line_fft_v<N, true>(v, p, xl, tw, u);
         }
-        float2 u[E];
-        reg_line_fft_v<N, true>(v, p, xl, tw, u);
         if (valid) {
+            const float a0 = after ? mk.wa[0] : 1.f;
             float2* y = Y + z * ystride + k1 + P1 * k2;
 #pragma unroll
             for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
-                for (int k = 0; k < N2; ++k) y[((p + N2 * j) + N1 * k) * s3] = u[j * N2 + k];
+                for (int kk = 0; kk < N2; ++kk) {
+                    const float2 w = u[j * N2 + kk];
+                    y[((p + N2 * j) + N1 * kk) * s3] = after ? c_scale(w, a0) : w;
+                }
         }
         __syncthreads();   // the exchange rows are reused by the next subband
     }
 }
 
 // Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
-// added into the accumulator with Kahan compensation (item order).  The
-// running sums and their compensations are loaded from acc / comp, carried in
-// registers or shared memory across the group's items, and stored back: one
-// round trip of both per group, so the compensation spans the whole synthesis
+// added into the accumulator with Kahan compensation.  The running sums and
+// their compensations are loaded from acc / comp, carried in registers or
+// shared memory across the group's items, and stored back: one round trip of
+// both per group, so the compensation spans the whole synthesis
 // (src/transforms/ns_surfacelet.jl:292, 355, 383 accumulate every subband
 // into one spectrum).
+//
+// A wedge plane constant along axis 3 commutes with the axis-3 FFT, so the
+// items that share plane b (and the group factor) are combined first,
+// sum_p wa_p(k1, k2) Y_pq, and transformed once: with nbq > 0 the chunk is
+// nbq plane-b wedges q times whole rows p (item t = p nbq + q); otherwise
+// every item is its own term.  Terms are added in q order.
 template <int N>
 __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(const float2* __restrict__ Y, long long ystride, int G,
                                                             int P1, int s3, BoxMap bx, NSMaskTables tb,
                                                             const NSItem* __restrict__ items, int item0, int synth,
                                                             float2* acc, float2* comp, const float2* __restrict__ tw,
-                                                            int nlines, long long ychs, long long achs) {
+                                                            int nlines, long long ychs, long long achs, int nbq) {
     using Ge = RegGeom<N>;
     constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP, E = Ge::M * Ge::N2;
     extern __shared__ float2 xch[];
@@ -285,22 +310,42 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
                 gf[j * N2 + k] = m0.low ? m0.lowc * m0.lowv[k3] : m0.m[k3 * si_nat];
             }
     }
-    for (int z = 0; z < G; ++z) {
-        L3LoadC ld{Y + z * ystride, 0, P1, s3, bx};
-        L3LoadC::Ctx lc{ld.src + k1 + P1 * k2};
+    const int rows = nbq > 0 ? G / nbq : 1;
+    const int nterms = nbq > 0 ? nbq : G;
+    const float2* yl = Y + k1 + P1 * k2;
+    for (int t = 0; t < nterms; ++t) {
+        // plane a constant along the line (directional item, tight or analysis masks): applied before the FFT
+        const NSItem* it0 = items + item0 + t;
+        const bool before = it0->kind == 0 && !(synth && !tb.tight) && it0->wa_hi != 2;
+        // the term: sum_p wa_p Y_pq (one item with weight 1 when plane a varies along the line; x 1 is exact)
+        const int nt = before ? rows : 1;
+        float2 v[N1];
+#pragma unroll 1
+        for (int pp = 0; pp < nt; ++pp) {
+            const int z = nbq > 0 ? pp * nbq + t : t;
+            const float az = before ? ns_wedge_a_line(tb, items + item0 + z, k1, k2) : 1.f;
+            const float2* yz = yl + z * ystride;
+#pragma unroll
+            for (int r = 0; r < N1; ++r) {
+                const float2 y = valid ? yz[(long long)(p + N2 * r) * s3] : make_float2(0.f, 0.f);
+                v[r] = pp == 0 ? c_scale(y, az) : make_float2(fmaf(y.x, az, v[r].x), fmaf(y.y, az, v[r].y));
+            }
+        }
         float2 u[E];
-        reg_line_fft<N, false>(ld, lc, valid, p, xl, tw, u);
-        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
+        reg_line_fft_v<N, false>(v, p, xl, tw, u);
+        // the term's first item carries plane b and the group factor
+        const NSMaskLine mk = ns_mask_line(tb, *it0, lnat, synth != 0);
         const bool wedges = !(mk.low || mk.plain);
 #pragma unroll
         for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
             for (int k = 0; k < N2; ++k) {
                 const int k3 = (p + N2 * j) + N1 * k;
-                const float m = wedges ? gf[j * N2 + k] * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]) : gf[j * N2 + k];
+                const float g = gf[j * N2 + k];
+                const float m = !wedges ? g : (before ? g * mk.wb[k3 * mk.wbs] : g * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]));
                 kahan_add(sum(j * N2 + k), cmp(j * N2 + k), c_scale(u[j * N2 + k], m));
             }
-        __syncthreads();   // the exchange rows are reused by the next item
+        __syncthreads();   // the exchange rows are reused by the next term
     }
     if (valid) {
 #pragma unroll
@@ -852,7 +897,7 @@ void line3(const NSPlan& P, const Load& ld, const Store& so, int nlines, int nz,
 
 template <int N>
 void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& bx, int i0, int synth, float2* acc,
-                       float2* comp, int nlines, int nch, long long ychs, long long achs, cudaStream_t st) {
+                       float2* comp, int nlines, int nch, long long ychs, long long achs, int nbq, cudaStream_t st) {
     using Ge = RegGeom<N>;
     static bool configured = false;
     if (!configured) {
@@ -865,14 +910,14 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
     int tok = prof_begin("ns_slab_accum_axis3", st);
     ns_slab_accum_kernel<N><<<grid, Ge::THREADS, accum_smem<N>(), st>>>(Y, P.SP, nz, P.P1, P.P1 * P.dims[1], bx, P.tb,
                                                                  P.items.as<NSItem>(), i0, synth, acc, comp,
-                                                                 P.ffts.at(P.dims[2])->sh.tw, nlines, ychs, achs);
+                                                                 P.ffts.at(P.dims[2])->sh.tw, nlines, ychs, achs, nbq);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
 }
 
 template <int N, int IPC>
 void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
-                           int nlines, int nch, long long xchs, long long ychs, cudaStream_t st) {
+                           int nlines, int nch, long long xchs, long long ychs, int nbq, cudaStream_t st) {
     using Ge = RegGeom<N>;
     static bool configured = false;
     if (!configured) {
@@ -885,7 +930,7 @@ void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, 
     int tok = prof_begin("ns_slab_mask_axis3", st);
     ns_slab_mask_group_kernel<N, IPC><<<grid, Ge::THREADS, Ge::SMEM, st>>>(
         X, P.P1, P.P1 * P.dims[1], bx, P.tb, P.items.as<NSItem>(), i0, nz, synth, Y, P.SP,
-        P.ffts.at(P.dims[2])->sh.tw, nlines, xchs, ychs);
+        P.ffts.at(P.dims[2])->sh.tw, nlines, xchs, ychs, nbq);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "ns_slab_mask_group_kernel launch");
 }
@@ -906,12 +951,31 @@ int mask_ipc(int nz) {
 
 template <int N>
 void launch_mask_group(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
-                       int nlines, int nch, long long xchs, long long ychs, cudaStream_t st) {
+                       int nlines, int nch, long long xchs, long long ychs, int nbq, cudaStream_t st) {
     switch (mask_ipc(nz)) {
-        case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, st); return;
-        case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, st); return;
-        default: launch_mask_group_ipc<N, 1>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, st); return;
+        case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
+        case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
+        default: launch_mask_group_ipc<N, 1>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
     }
+}
+
+// Items [i0, i0 + nz) as nbq plane-b wedges times whole rows of plane-a
+// wedges constant along axis 3 (item t = p nbq + q, one mask group): nbq,
+// else 0.  Only then do the axis-3 passes share FFTs between items.
+int chunk_nbq(const NSPlan& P, int i0, int nz, bool synth_masks) {
+    if (nz < 2 || (synth_masks && !P.p.tight)) return 0;
+    const NSItem& f = P.items_host[i0];
+    if (f.kind != 0 || f.wa_hi == 2) return 0;
+    int nb = 1;
+    while (nb < nz && P.items_host[i0 + nb].wb_off != f.wb_off) ++nb;
+    if (nz % nb != 0) return 0;
+    for (int t = 0; t < nz; ++t) {
+        const NSItem& it = P.items_host[i0 + t];
+        if (it.kind != 0 || it.g != f.g || it.wa_hi == 2 || it.wb_off != P.items_host[i0 + t % nb].wb_off ||
+            it.wa_off != P.items_host[i0 + (t / nb) * nb].wa_off)
+            return 0;
+    }
+    return nb;
 }
 
 // Algorithmic bytes of one box of a spectrum (complex float32 bins).
@@ -970,14 +1034,15 @@ void slab_mask_pass(NSPlan& P, const float2* X, int i0, int nz, bool synth_masks
     prof_bytes("ns_slab_mask_axis3", nch * (1.5 * box_bytes(P, b) + nz * box_bytes(P, b)));
     const int nl = b.nk1 * b.nk2, sy = synth_masks ? 1 : 0;
     const long long xc = P.SP, yc = ych_stride(P);
+    const int nbq = chunk_nbq(P, i0, nz, synth_masks);
     switch (P.dims[2]) {
-        case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
-        case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
-        case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
-        case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
-        case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
-        case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
-        case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, st); return;
+        case 16: launch_mask_group<16>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
+        case 32: launch_mask_group<32>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
+        case 64: launch_mask_group<64>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
+        case 96: launch_mask_group<96>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
+        case 128: launch_mask_group<128>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
+        case 160: launch_mask_group<160>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
+        case 256: launch_mask_group<256>(P, X, Y, nz, bx, i0, sy, nl, nch, xc, yc, nbq, st); return;
     }
     throw ArgError("no register line pass for axis 3 of this size");
 }
@@ -994,14 +1059,15 @@ void slab_accum_pass(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc
     const int nl = b.nk1 * b.nk2;
     const int sy = analysis_masks ? 0 : 1;
     const long long yc = ych_stride(P), ac = P.SP;
+    const int nbq = chunk_nbq(P, i0, nz, !analysis_masks);
     switch (P.dims[2]) {
-        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
-        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
-        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
-        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
-        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
-        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
-        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, st); return;
+        case 16: launch_slab_accum<16>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
+        case 32: launch_slab_accum<32>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
+        case 64: launch_slab_accum<64>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
+        case 96: launch_slab_accum<96>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
+        case 128: launch_slab_accum<128>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
+        case 160: launch_slab_accum<160>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
+        case 256: launch_slab_accum<256>(P, Y, nz, bx, i0, sy, acc, comp, nl, nch, yc, ac, nbq, st); return;
     }
     throw ArgError("no register line pass for axis 3 of this size");
 }

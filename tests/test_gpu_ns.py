@@ -8,6 +8,7 @@ reference asserts it (complex = real + i imag, streaming = materialized).
 
 import numpy as np
 import pytest
+import torch
 
 from conftest import gpu_available
 from oracle import ns as N
@@ -188,15 +189,25 @@ def test_streaming_synthesis_stages_mask_groups(sfl, pipeline, dims):
         assert torch.equal(y2, y), g
 
 
-def test_group_size_does_not_change_results(sfl):
-    dims = (20, 16, 12)
+@pytest.mark.parametrize("dims,pipeline", [((20, 16, 12), "lines"), ((64, 64, 32), "slabs")])
+def test_group_size_does_not_change_results(sfl, dims, pipeline):
+    """Analysis is the same bit for bit at every group size.  Synthesis on the
+    slab pipeline combines the subbands that share a plane-b wedge before their
+    axis-3 FFT when a chunk holds whole rows of them, so other chunkings round
+    differently (float32 rounding level)."""
     t = sfl.NSSurfacelet(scales=2, direction_levels=[2, 3], bernstein_order=6)
     x = sfl.to_device(np.random.default_rng(5).standard_normal(dims).astype(np.float32))
     a = sfl.make_workspace(t, "float32", dims)
     b = sfl.make_workspace(t, "float32", dims, group=3)
+    a.set_pipeline(pipeline)
+    b.set_pipeline(pipeline)
     ca, cb = sfl.analyze(a, x), sfl.analyze(b, x)
     assert bool((ca == cb).all())
-    assert bool((sfl.synthesize(a, ca) == sfl.synthesize(b, ca)).all())
+    ya, yb = sfl.synthesize(a, ca), sfl.synthesize(b, ca)
+    if pipeline == "lines":
+        assert bool((ya == yb).all())
+    else:
+        assert float(torch.linalg.vector_norm(ya - yb) / torch.linalg.vector_norm(ya)) <= 1e-6
 
 
 def test_pipeline_selection_is_validated(sfl):
