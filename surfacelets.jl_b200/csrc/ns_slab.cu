@@ -17,7 +17,8 @@
 //     slab pass  per n3: R2C along axis 1 (two columns at a time), FFT_2 of
 //                the rows in the box -> Y_s;
 //     line pass  FFT_3 of Y_s times M_s, summed over the subbands of one mask
-//                group in registers, one accumulator round trip per group;
+//                group in registers, then one Kahan-compensated step into the
+//                accumulator (a round trip of it and its compensation per group);
 //     then the irfft of the accumulator (line pass and slab pass, no mask).
 //
 // Support boxes: the group factor B_j of scale j is a product of per-axis
@@ -129,14 +130,9 @@ constexpr int accum_minb() { return (N == 96 || N == 160 || N >= 256) ? 1 : 2; }
 // Accumulation lengths whose sums go to shared memory (their register form spills).
 template <int N>
 constexpr bool accum_sums_shared() { return N == 96 || N == 128 || N == 160; }
-// Lengths whose Kahan compensations go to shared memory beside the sums (160: the exchange rows and the
-// sums leave no room, so its compensations stay in registers).
-template <int N>
-constexpr bool accum_comps_shared() { return N == 96 || N == 128; }
 template <int N>
 constexpr size_t accum_smem() {
-    constexpr size_t plane = sizeof(float2) * RegGeom<N>::M * RegGeom<N>::N2 * 256;
-    return RegGeom<N>::SMEM + (accum_sums_shared<N>() ? plane : 0) + (accum_comps_shared<N>() ? plane : 0);
+    return RegGeom<N>::SMEM + (accum_sums_shared<N>() ? sizeof(float2) * RegGeom<N>::M * RegGeom<N>::N2 * 256 : 0);
 }
 
 // Analysis line pass over IPC subbands of one mask group per CTA: a line's X
@@ -234,12 +230,11 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
 }
 
 // Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
-// added into the accumulator with Kahan compensation.  The running sums and
-// their compensations are loaded from acc / comp, carried in registers or
-// shared memory across the group's items, and stored back: one round trip of
-// both per group, so the compensation spans the whole synthesis
-// (src/transforms/ns_surfacelet.jl:292, 355, 383 accumulate every subband
-// into one spectrum).
+// summed in float32 over the launch's terms, then added into the accumulator
+// with one Kahan step against the compensation grid comp: the compensation
+// carries across launches, so the sum over the mask groups of the whole
+// synthesis is compensated (src/transforms/ns_surfacelet.jl:292, 355, 383
+// accumulate every subband into one spectrum).
 //
 // A wedge plane constant along axis 3 commutes with the axis-3 FFT, so the
 // items that share plane b (and the group factor) are combined first,
@@ -264,38 +259,20 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
     const bool valid = l < nlines;
     int k1 = 0, k2 = 0;
     if (valid) bx.k12(l, k1, k2);
-    float2* a = acc + k1 + P1 * k2;
-    float2* ca = comp + k1 + P1 * k2;
     float2* xl = xch + lp * Ge::XLINE;
-    // the line's sums and compensations: in registers, or (lengths whose registers would spill) in shared
-    // memory after the exchange rows, value q of thread t at [q * 256 + t] (sums), then the same for the
-    // compensations
+    // the launch's sums: in registers, or (lengths whose registers would spill) in shared memory after the
+    // exchange rows, value q of thread t at [q * 256 + t]
     constexpr bool kSumsShared = accum_sums_shared<N>();
-    constexpr bool kCompsShared = accum_comps_shared<N>();
     float2 sr[kSumsShared ? 1 : E];
-    float2 cr[kCompsShared ? 1 : E];
     float2* ss = xch + LP * Ge::XLINE + tid;
-    float2* cs = ss + (kSumsShared ? E * Ge::THREADS : 0);
     auto sum = [&](int q) -> float2& {
         if constexpr (kSumsShared)
             return ss[q * Ge::THREADS];
         else
             return sr[q];
     };
-    auto cmp = [&](int q) -> float2& {
-        if constexpr (kCompsShared)
-            return cs[q * Ge::THREADS];
-        else
-            return cr[q];
-    };
 #pragma unroll
-    for (int j = 0; j < Ge::M; ++j)
-#pragma unroll
-        for (int k = 0; k < N2; ++k) {
-            const long long o = (long long)((p + N2 * j) + N1 * k) * s3;
-            sum(j * N2 + k) = valid ? a[o] : make_float2(0.f, 0.f);
-            cmp(j * N2 + k) = valid ? ca[o] : make_float2(0.f, 0.f);
-        }
+    for (int q = 0; q < E; ++q) sum(q) = make_float2(0.f, 0.f);
     const long long si_nat = (long long)tb.h1 * tb.n2;
     const int lnat = k1 + tb.h1 * k2;
     // the group factor of the line (group table, bandpass table or the lowpass factors), once for all items
@@ -343,18 +320,23 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
                 const int k3 = (p + N2 * j) + N1 * k;
                 const float g = gf[j * N2 + k];
                 const float m = !wedges ? g : (before ? g * mk.wb[k3 * mk.wbs] : g * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]));
-                kahan_add(sum(j * N2 + k), cmp(j * N2 + k), c_scale(u[j * N2 + k], m));
+                float2& tsum = sum(j * N2 + k);
+                tsum = c_add(tsum, c_scale(u[j * N2 + k], m));
             }
         __syncthreads();   // the exchange rows are reused by the next term
     }
     if (valid) {
+        float2* a = acc + k1 + P1 * k2;
+        float2* ca = comp + k1 + P1 * k2;
 #pragma unroll
         for (int j = 0; j < Ge::M; ++j)
 #pragma unroll
             for (int k = 0; k < N2; ++k) {
                 const long long o = (long long)((p + N2 * j) + N1 * k) * s3;
-                a[o] = sum(j * N2 + k);
-                ca[o] = cmp(j * N2 + k);
+                float2 sv = a[o], cv = ca[o];
+                kahan_add(sv, cv, sum(j * N2 + k));
+                a[o] = sv;
+                ca[o] = cv;
             }
     }
 }

@@ -48,6 +48,6 @@ def test_timed_out_wait_is_reported_once_by_the_next_call(sfl, pipeline):
 
 
 def test_selftest_needs_an_ns_plan(sfl):
-    ws = sfl.make_workspace(sfl.Surfacelet(scales=1, direction_levels=[1]), "float32", (32, 32, 32))
+    ws = sfl.make_workspace(sfl.Surfacelet(scales=1, direction_levels=[1]), "float32", (48, 48, 48))
     rc = sfl.lib.sfl_plan_selftest_wait(ws._h, None)
     assert rc == sfl._lib.SFL_ERR_ARGUMENT

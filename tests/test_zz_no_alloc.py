@@ -86,6 +86,7 @@ def test_static_scratch_rejects_bad_arguments(sfl, case):
         ws = sfl.make_workspace(sfl.NSSurfacelet(scales=2, direction_levels=[1, 1], bernstein_order=6), "complex64", dims)
         msg, i = "real", 2
     elif case == "decimated":
+        dims = (48, 48, 48)         # the default pyramid_ratio 1.5 needs lengths divisible by 3
         ws = sfl.make_workspace(sfl.Surfacelet(scales=1, direction_levels=[1]), "float32", dims)
         msg, i = "NSSurfacelet plans only", 2
     else:
