@@ -297,6 +297,13 @@ int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const
  * n2 n3 floats to the host buffer out (when not NULL) and H to *count.
  * Equal bit for bit to the float64 host design rounded to float32. */
 int sfl_ns_plan_table(sfl_plan* plan, const char* name, int32_t index, float* out, int64_t* count);
+/* The float32 tables a Surfacelet plan holds on the device (composed there in
+ * float64 from the host's separable factors, src/directional/ritf.jl:89-108,
+ * src/directional/irc.jl:49-67): "ritf" (V_K on the half-K grid; index =
+ * level*3 + K-1) and "irc" (one stage's slice plane as re/im pairs; index as
+ * in sfl_surf_design_table).  Writes the float count to *count and the values
+ * to the host buffer out when not NULL.  No counterpart in the reference. */
+int sfl_surf_plan_table(sfl_plan* plan, const char* name, int32_t index, float* out, int64_t* count);
 
 /* ── Soft-threshold denoiser (NSSurfacelet and NDFB plans, Float32) ─────
  * No counterpart in the reference.  y = synthesize(soft(analyze(x), tau)),

@@ -106,6 +106,7 @@ SIGNATURES = {
     "sfl_surf_design_table": (C.c_int, [C.POINTER(SurfParams), Dims, C.c_char_p, C.c_int32,
                                         C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "sfl_ns_plan_table": (C.c_int, [P, C.c_char_p, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_int64)]),
+    "sfl_surf_plan_table": (C.c_int, [P, C.c_char_p, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_int64)]),
     "sfl_ns_denoise": (C.c_int, [P, P, P, P, P]),
     "sfl_ns_spectrum_elems": (C.c_int, [P, C.POINTER(C.c_int64)]),
     "sfl_ns_stream_order": (C.c_int, [P, C.POINTER(C.c_int32)]),

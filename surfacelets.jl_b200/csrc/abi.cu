@@ -864,6 +864,23 @@ int sfl_ns_plan_table(sfl_plan* plan, const char* name, int32_t index, float* ou
     });
 }
 
+int sfl_surf_plan_table(sfl_plan* plan, const char* name, int32_t index, float* out, int64_t* count) {
+    return guarded([&] {
+        need(plan, "plan");
+        need(name, "name");
+        need(count, "count");
+        if (plan->impl.kind != SFL_KIND_DECIMATED) throw sfl::ArgError("sfl_surf_plan_table takes Surfacelet plans");
+        long long n = 0;
+        const float* src = sfl::dec_plan_table(*plan->impl.dec, name, index, &n);
+        *count = n;
+        if (out)
+            on_device(plan, [&] {
+                sfl::cuda_check(cudaMemcpy(out, src, sizeof(float) * n, cudaMemcpyDeviceToHost), "table readback");
+            });
+        return SFL_OK;
+    });
+}
+
 int sfl_surf_design_table(const sfl_surf_params* p, const int32_t dims[3], const char* name, int32_t index,
                           double* out, int64_t* count) {
     return guarded([&] {

@@ -57,6 +57,28 @@ struct DecPlan {
 
 void DecPlanDeleter::operator()(DecPlan* d) const { delete d; }
 const SurfDesign& dec_design(const DecPlan& d) { return d.design; }
+
+// A table the plan holds on the device, as floats: "ritf" (index = level * 3 +
+// K - 1: V_K) or "irc" (index = ((level * 3 + K - 1) * 32 + stage) * 4 +
+// which; float2 values as re/im pairs).
+const float* dec_plan_table(const DecPlan& d, const std::string& name, int index, long long* count) {
+    if (name == "ritf") {
+        const int lv = index / 3, K = index % 3;
+        if (index < 0 || lv >= (int)d.lv.size()) throw ArgError("table index out of range");
+        const int* h = d.lv[lv]->hd[K];
+        *count = (long long)h[0] * h[1] * h[2];
+        return d.lv[lv]->V[K].as<float>();
+    }
+    if (name == "irc") {
+        const int which = index % 4, stage = (index / 4) % 32, K = (index / 128) % 3, lv = index / 384;
+        if (index < 0 || lv >= (int)d.lv.size() || stage >= (int)d.lv[lv]->stages[K].size())
+            throw ArgError("table index out of range");
+        const DecStageDev& sd = d.lv[lv]->stages[K][stage];
+        *count = (long long)(sd.f[which].bytes / sizeof(float));
+        return sd.f[which].as<float>();
+    }
+    throw ArgError("unknown table " + name);
+}
 int dec_nsubbands(const DecPlan& d) { return (int)d.design.sizes.size(); }
 long long dec_ncoeffs(const DecPlan& d) { return d.ncoef; }
 void dec_subband_info(const DecPlan& d, int i, int shape[3], long long* offset) {
@@ -521,7 +543,7 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
     for (int d = 0; d < 3; ++d)
         if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
     std::unique_ptr<DecPlan> D(new DecPlan);
-    D->design = surf_design(p, dims);
+    D->design = surf_design(p, dims, false);   // factors only: the tables are composed on the device
     const SurfDesign& S = D->design;
     for (int d = 0; d < 3; ++d) D->dims[d] = dims[d];
     D->nch = dtype == SFL_COMPLEX64 ? 2 : 1;
@@ -560,21 +582,26 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
             upload_vec(L->hw, hw);
         }
         int first = S.level_first[j];   // 0-based index of the level's first subband
+        {
+            float* Vp[3];
+            for (int K = 0; K < 3; ++K) {
+                for (int d = 0; d < 3; ++d) L->hd[K][d] = d == K ? sc.n[K] / 2 + 1 : sc.n[d];
+                L->V[K].alloc(sizeof(float) * (size_t)L->hd[K][0] * L->hd[K][1] * L->hd[K][2]);
+                Vp[K] = L->V[K].as<float>();
+            }
+            ritf_masks_device(sc.n, sc.P, Vp, 0);
+        }
         for (int K = 0; K < 3; ++K) {
-            for (int d = 0; d < 3; ++d) L->hd[K][d] = d == K ? sc.n[K] / 2 + 1 : sc.n[d];
-            std::vector<float> vf(sc.V[K].begin(), sc.V[K].end());
-            upload_vec(L->V[K], vf);
             for (const IRCStage& st : sc.stages[K]) {
                 DecStageDev sd;
                 sd.m = st.m - 1;
                 sd.b = st.b;
-                const std::vector<std::complex<double>>* src[4] = {&st.ana[0], &st.ana[1], &st.syn[0], &st.syn[1]};
+                float2* fp[4];
                 for (int w = 0; w < 4; ++w) {
-                    std::vector<float2> f(src[w]->size());
-                    for (size_t i = 0; i < f.size(); ++i)
-                        f[i] = make_float2((float)(*src[w])[i].real(), (float)(*src[w])[i].imag());
-                    upload_vec(sd.f[w], f);
+                    sd.f[w].alloc(sizeof(float2) * (size_t)st.fac.nKh * st.fac.nm);
+                    fp[w] = sd.f[w].as<float2>();
                 }
+                irc_slices_device(st.fac, fp, 0);
                 L->stages[K].push_back(std::move(sd));
             }
             int nb = 1;

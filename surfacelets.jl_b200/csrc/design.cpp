@@ -716,15 +716,14 @@ static double ritf_diamond(const std::vector<double>& w, double a, double b) {
     return cea * ceb + coa * cob;
 }
 
-// src/directional/ritf.jl:76-108: V_K on the half-K grid.
-void ritf_masks(const int n[3], int msize, double beta, int lambda, std::vector<double> V[3]) {
+// src/directional/ritf.jl:76-84: the planes D(w_K + pi, w_m)^lambda, m != K.
+void ritf_planes(const int n[3], int msize, double beta, int lambda, std::vector<double> P[3][3]) {
     for (int d = 0; d < 3; ++d)
         if (n[d] % 2 != 0) throw ArgError("the hourglass stage needs even dimensions, got " + fmt_dims(n));
     std::vector<double> w = ritf_window(msize, beta);
-    // planes P[K][m] (nK x nm) = D(w_K + pi, w_m)^lambda
-    std::vector<double> P[3][3];
     for (int K = 0; K < 3; ++K)
         for (int m = 0; m < 3; ++m) {
+            P[K][m].clear();
             if (m == K) continue;
             int nK = n[K], nm = n[m];
             P[K][m].resize((size_t)nK * nm);
@@ -735,6 +734,12 @@ void ritf_masks(const int n[3], int msize, double beta, int lambda, std::vector<
                     P[K][m][k + (size_t)nK * l] = std::pow(ritf_diamond(w, a, b), lambda);
                 }
         }
+}
+
+// src/directional/ritf.jl:89-108: V_K on the half-K grid.  The order of the
+// operations is the device kernel's (dec_design.cu): h_K = P_a P_b (m
+// ascending), tot = (h_1 + h_2) + h_3, V = sqrt((3 h_K) / tot).
+void ritf_compose(const int n[3], const std::vector<double> P[3][3], std::vector<double> V[3]) {
     auto hg = [&](int K, int i0, int i1, int i2) {
         int idx[3] = {i0, i1, i2};
         double acc = 1.0;
@@ -759,27 +764,89 @@ void ritf_masks(const int n[3], int msize, double beta, int lambda, std::vector<
     }
 }
 
+void ritf_masks(const int n[3], int msize, double beta, int lambda, std::vector<double> V[3]) {
+    std::vector<double> P[3][3];
+    ritf_planes(n, msize, beta, lambda, P);
+    ritf_compose(n, P, V);
+}
+
 // Checkerboard responses: src/filters/checkerboard.jl:71-91
 static double cbd_b(const std::vector<double>& t, double w) {
     double s = 0;
     for (size_t i = 0; i < t.size(); ++i) s += t[i] * std::sin((2.0 * (i + 1) - 1) * w);
     return 2 * s;
 }
-static std::complex<double> cbd_response(const std::vector<double>& t, bool synthesis, int chan, double w1,
-                                         double w2) {
-    double B = -cbd_b(t, w1) * cbd_b(t, w2);
-    double r = 1 / std::sqrt(2.0);
-    if (!synthesis) {
-        if (chan == 0) return {r * (1 + B), 0.0};
-        return std::polar(1.0, w2) * (r * (2 - B - B * B));
-    }
-    if (chan == 0) return {r * (2 + B - B * B), 0.0};
-    return std::polar(1.0, -w2) * (r * (1 - B));
+
+// src/directional/irc.jl:49-67 with the ladder responses of
+// src/filters/checkerboard.jl:80-91: stage le on axis m of length nm splits
+// it into groups of W = nm >> (le - 1) bins; bin c = g W + l has
+// w_m = 2 pi l / W + sf_g w_K, sf_g = 2^(le-1) - 1 - 2g.
+IRCFactors irc_factors(int nKh, int nK, int nm, int le, int bo) {
+    const std::vector<double>& t = cbd_ladder(bo);
+    IRCFactors F;
+    F.nKh = nKh;
+    F.nm = nm;
+    F.W = nm >> (le - 1);
+    F.ng = nm / F.W;
+    F.nq = (int)t.size();
+    F.t = t;
+    F.r = 1 / std::sqrt(2.0);
+    F.bK.resize(nKh);
+    for (int k = 0; k < nKh; ++k) F.bK[k] = cbd_b(t, 2 * kPi * k / nK);
+    F.sth.resize((size_t)F.nq * F.W);
+    F.cth.resize((size_t)F.nq * F.W);
+    for (int i = 0; i < F.nq; ++i)
+        for (int l = 0; l < F.W; ++l) {
+            const double th = (2.0 * (i + 1) - 1) * (2 * kPi * l / F.W);
+            F.sth[(size_t)i * F.W + l] = std::sin(th);
+            F.cth[(size_t)i * F.W + l] = std::cos(th);
+        }
+    F.sph.resize((size_t)F.nq * F.ng * nKh);
+    F.cph.resize((size_t)F.nq * F.ng * nKh);
+    for (int i = 0; i < F.nq; ++i)
+        for (int g = 0; g < F.ng; ++g) {
+            const int sf = (1 << (le - 1)) - 1 - 2 * g;
+            for (int k = 0; k < nKh; ++k) {
+                const double ph = (2.0 * (i + 1) - 1) * (sf * (2 * kPi * k / nK));
+                F.sph[((size_t)i * F.ng + g) * nKh + k] = std::sin(ph);
+                F.cph[((size_t)i * F.ng + g) * nKh + k] = std::cos(ph);
+            }
+        }
+    return F;
 }
 
-// src/directional/irc.jl:49-67, 275-290 (file numbering)
-std::vector<IRCStage> irc_stages(const int hdims[3], int nK, int K, const int levels[3], int bo) {
-    const std::vector<double>& t = cbd_ladder(bo);
+// B = -b(w_K) b(w_m); analysis H0 = (1 + B)/sqrt2, H1 = e^{i w_m} (2 - B - B^2)/sqrt2,
+// both x 0.5; synthesis G0 = (2 + B - B^2)/sqrt2, G1 = e^{-i w_m} (1 - B)/sqrt2.
+// Every step below is one IEEE operation, in the order dec_design.cu uses.
+void irc_slice_values(const IRCFactors& F, int k, int c, std::complex<double> out[4]) {
+    const int g = c / F.W, l = c - g * F.W;
+    double s = 0, sw = 0, cw = 0;
+    for (int i = 0; i < F.nq; ++i) {
+        const double st = F.sth[(size_t)i * F.W + l], ct = F.cth[(size_t)i * F.W + l];
+        const size_t q = ((size_t)i * F.ng + g) * F.nKh + k;
+        const double sp = F.sph[q], cp = F.cph[q];
+        const double sq = st * cp + ct * sp;   // sin(q_i w_m)
+        if (i == 0) {
+            sw = sq;
+            cw = ct * cp - st * sp;             // cos(w_m)
+        }
+        s = s + F.t[i] * sq;
+    }
+    const double bm = 2 * s;
+    const double B = -F.bK[k] * bm;
+    const double B2 = B * B;
+    const double h0 = F.r * (1 + B);
+    const double h1 = F.r * ((2 - B) - B2);
+    const double g0 = F.r * ((2 + B) - B2);
+    const double g1 = F.r * (1 - B);
+    out[0] = {0.5 * h0, 0.0};
+    out[1] = {0.5 * (cw * h1), 0.5 * (sw * h1)};
+    out[2] = {g0, 0.0};
+    out[3] = {cw * g1, -(sw * g1)};
+}
+
+// src/directional/irc.jl:76-91: the stages of hourglass K, axes m ascending.
+std::vector<IRCStage> irc_stages(const int hdims[3], int nK, int K, const int levels[3], int bo, bool values) {
     std::vector<IRCStage> out;
     for (int m = 1; m <= 3; ++m) {
         if (m == K) continue;
@@ -792,23 +859,23 @@ std::vector<IRCStage> irc_stages(const int hdims[3], int nK, int K, const int le
             IRCStage st;
             st.m = m;
             st.b = hdims[m - 1] >> le;
-            int nKh = hdims[K - 1], nm = hdims[m - 1];
-            int W = nm >> (le - 1);
-            for (int c = 0; c < 2; ++c) {
-                st.ana[c].resize((size_t)nKh * nm);
-                st.syn[c].resize((size_t)nKh * nm);
-            }
-            for (int cc = 0; cc < nm; ++cc) {
-                int g = cc / W, l = cc % W;
-                int sf = (1 << (le - 1)) - 1 - 2 * g;
-                for (int k = 0; k < nKh; ++k) {
-                    double wK = 2 * kPi * k / nK;
-                    double wm = 2 * kPi * l / W + sf * wK;
-                    for (int c = 0; c < 2; ++c) {
-                        st.ana[c][k + (size_t)nKh * cc] = 0.5 * cbd_response(t, false, c, wK, wm);
-                        st.syn[c][k + (size_t)nKh * cc] = 1.0 * cbd_response(t, true, c, wK, wm);
-                    }
+            const int nKh = hdims[K - 1], nm = hdims[m - 1];
+            st.fac = irc_factors(nKh, nK, nm, le, bo);
+            if (values) {
+                for (int c = 0; c < 2; ++c) {
+                    st.ana[c].resize((size_t)nKh * nm);
+                    st.syn[c].resize((size_t)nKh * nm);
                 }
+                for (int cc = 0; cc < nm; ++cc)
+                    for (int k = 0; k < nKh; ++k) {
+                        std::complex<double> v[4];
+                        irc_slice_values(st.fac, k, cc, v);
+                        const size_t e = k + (size_t)nKh * cc;
+                        st.ana[0][e] = v[0];
+                        st.ana[1][e] = v[1];
+                        st.syn[0][e] = v[2];
+                        st.syn[1][e] = v[3];
+                    }
             }
             out.push_back(std::move(st));
         }
@@ -817,7 +884,7 @@ std::vector<IRCStage> irc_stages(const int hdims[3], int nK, int K, const int le
 }
 
 // src/transforms/surfacelet.jl:73-102, 136-149
-SurfDesign surf_design(const sfl_surf_params& p, const int dims[3]) {
+SurfDesign surf_design(const sfl_surf_params& p, const int dims[3], bool tables) {
     surf_check_params(p);
     SurfDesign S;
     for (int d = 0; d < 3; ++d) S.dims[d] = dims[d];
@@ -829,11 +896,12 @@ SurfDesign surf_design(const sfl_surf_params& p, const int dims[3]) {
         ScaleDesign sc;
         for (int d = 0; d < 3; ++d) sc.n[d] = S.pyramid[j - 1].n[d];
         levels_of(p, J - j, sc.lv);
-        ritf_masks(sc.n, p.diamond_length, p.kaiser_beta, p.diamond_power, sc.V);
+        ritf_planes(sc.n, p.diamond_length, p.kaiser_beta, p.diamond_power, sc.P);
+        if (tables) ritf_compose(sc.n, sc.P, sc.V);
         for (int K = 1; K <= 3; ++K) {
             int hd[3] = {sc.n[0], sc.n[1], sc.n[2]};
             hd[K - 1] = sc.n[K - 1] / 2 + 1;
-            sc.stages[K - 1] = irc_stages(hd, sc.n[K - 1], K, sc.lv[K - 1], p.checkerboard_order);
+            sc.stages[K - 1] = irc_stages(hd, sc.n[K - 1], K, sc.lv[K - 1], p.checkerboard_order, tables);
         }
         S.scales.push_back(std::move(sc));
     }

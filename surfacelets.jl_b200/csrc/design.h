@@ -103,18 +103,37 @@ struct PyrLevel {
     std::vector<double> prof[3];
 };
 
+// The separable factors of one IRC stage's filter slices
+// (src/directional/irc.jl:49-67, the ladder filters of
+// src/filters/checkerboard.jl:71-91): b(w) = 2 sum_i t_i sin(q_i w), q_i =
+// 2i + 1, at w_K = 2 pi k / n_K and at w_m = theta_l + phi_{g,k} with
+// theta_l = 2 pi l / W and phi_{g,k} = sf_g w_K.  sin(q_i w_m) and cos(w_m)
+// come from these 1-D tables by angle addition, so every later step is an
+// exact IEEE multiply or add: the host (irc_slice_values) and the device
+// (dec_design.cu) give the same float64 values bit for bit.
+struct IRCFactors {
+    int nKh = 0, nm = 0, W = 0, ng = 0, nq = 0;
+    double r = 0;                    // 1/sqrt(2)
+    std::vector<double> t;           // ladder taps t_i
+    std::vector<double> bK;          // b(w_K), k < nKh
+    std::vector<double> sth, cth;    // sin, cos(q_i theta_l): [i * W + l]
+    std::vector<double> sph, cph;    // sin, cos(q_i phi_{g,k}): [(i * ng + g) * nKh + k]
+};
+
 struct IRCStage {
     int m = 0;      // 1-based axis decimated
     int b = 0;      // block size after the stage
+    IRCFactors fac;
     // (K-half, m) planes, entry [k + nKh * c]: analysis channel 0/1 (x 0.5),
-    // synthesis channel 0/1.
+    // synthesis channel 0/1 (filled only when the host tables are asked for).
     std::vector<std::complex<double>> ana[2], syn[2];
 };
 
 struct ScaleDesign {
     int n[3];
     int lv[3][3];                  // [K][m]
-    std::vector<double> V[3];      // V_K on the half-K grid, column-major
+    std::vector<double> P[3][3];   // ritf diamond planes [K][m] (n_K x n_m, k fastest), m != K
+    std::vector<double> V[3];      // V_K on the half-K grid, column-major (host tables only)
     std::vector<IRCStage> stages[3];
 };
 
@@ -135,8 +154,19 @@ void surf_check_size(const sfl_surf_params& p, const int dims[3]);
 std::vector<std::array<int, 3>> surf_layout_sizes(const sfl_surf_params& p, const int dims[3]);
 int surf_nsubbands_scale(const int lv[3][3]);
 std::vector<PyrLevel> fourier_pyramid(const int dims[3], int J, double mode);
+// The 2-D factors of the ritf masks: P[K][m] = D(w_K + pi, w_m)^lambda on
+// (n_K, n_m), m != K (src/directional/ritf.jl:58-84).
+void ritf_planes(const int n[3], int msize, double beta, int lambda, std::vector<double> P[3][3]);
+// V_K = sqrt(3 h_K / (h_1 + h_2 + h_3)), h_K the product of P[K][m] over m != K
+// (src/directional/ritf.jl:89-108), from the planes.
+void ritf_compose(const int n[3], const std::vector<double> P[3][3], std::vector<double> V[3]);
 void ritf_masks(const int n[3], int msize, double beta, int lambda, std::vector<double> V[3]);
-std::vector<IRCStage> irc_stages(const int hdims[3], int nK, int K, const int levels[3], int bo);
-SurfDesign surf_design(const sfl_surf_params& p, const int dims[3]);
+IRCFactors irc_factors(int nKh, int nK, int nm, int le, int bo);
+// Slice values at (k, c): analysis channel 0/1 (x 0.5), synthesis channel 0/1.
+void irc_slice_values(const IRCFactors& F, int k, int c, std::complex<double> out[4]);
+std::vector<IRCStage> irc_stages(const int hdims[3], int nK, int K, const int levels[3], int bo, bool values = true);
+// tables = false: the pyramid, layout, ritf planes and IRC factors only (the
+// device composes V_K and the slices from them, dec_design.cu).
+SurfDesign surf_design(const sfl_surf_params& p, const int dims[3], bool tables = true);
 
 }  // namespace sfl

@@ -228,6 +228,11 @@ int ns_next_chunk(const NSPlan& P, int i0);
 void ns_analyze_range(NSPlan& P, const float2* X, float* vol, ZMap vz, int es, int i0, int nz, bool synth_masks,
                       cudaStream_t st);
 void ns_acc_clear(NSPlan& P, float2* acc, float2* comp, cudaStream_t st);
+// Decimated design tables composed on the device from their host factors
+// (dec_design.cu): V_K into V[K] (float32, half-K grids) and one IRC stage's
+// four slice planes (float2, nKh x nm).
+void ritf_masks_device(const int n[3], const std::vector<double> P[3][3], float* const V[3], cudaStream_t st);
+void irc_slices_device(const IRCFactors& F, float2* const out[4], cudaStream_t st);
 // The plan's Kahan compensation grid of channel ch (spectrum-sized).
 float2* ns_comp_grid(NSPlan& P, int ch);
 // Runs out one bounded mbarrier wait on purpose (no copy in flight) so that
@@ -266,5 +271,6 @@ void dec_synthesize(DecPlan& d, const void* c, void* x, cudaStream_t st);
 void dec_adjoint_analyze(DecPlan& d, const void* c, void* x, cudaStream_t st);
 void dec_adjoint_synthesize(DecPlan& d, const void* x, void* c, cudaStream_t st);
 const SurfDesign& dec_design(const DecPlan& d);
+const float* dec_plan_table(const DecPlan& d, const std::string& name, int index, long long* count);
 
 }  // namespace sfl
