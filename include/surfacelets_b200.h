@@ -195,8 +195,8 @@ int sfl_plan_set_group(sfl_plan* plan, int32_t group);
  *     along axis 3 plus one pass per axis-3 slab, skipping the zero rows and
  *     columns of band-limited masks.
  *   LINES (default elsewhere): one line pass per axis.
- *   PLANES: a pass along axis 1 plus a 2-D pass per axis-1 frequency plane
- *     (axes 2 and 3 of length 64, 96 or 128).
+ *   PLANES: retired (the plane-major pipeline was slower than SLABS at every
+ *     size it supported); selecting it returns SFL_ERR_ARGUMENT.
  * Not while a streaming pass is open. */
 #define SFL_PIPELINE_LINES 0
 #define SFL_PIPELINE_PLANES 1

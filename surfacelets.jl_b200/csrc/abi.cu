@@ -150,13 +150,13 @@ void check_timeout(const sfl_plan* plan) {
 void ns_apply(sfl::NSPlan& N, int pipeline, int group) {
     cudaDeviceSynchronize();
     if (pipeline == SFL_PIPELINE_LINES) {
-        N.plane = false;
         if (N.slab) {
             N.slab = false;
             sfl::ns_alloc_scratch(N);
         }
     } else if (pipeline == SFL_PIPELINE_PLANES) {
-        sfl::ns_use_planes(N);
+        throw sfl::ArgError("the plane-major pipeline was retired: the slab pipeline is faster at every size it "
+                            "supported");
     } else if (pipeline == SFL_PIPELINE_SLABS) {
         sfl::ns_use_slabs(N);
     } else {
@@ -169,7 +169,7 @@ void ns_apply(sfl::NSPlan& N, int pipeline, int group) {
 }
 
 int ns_pipeline_of(const sfl::NSPlan& N) {
-    return N.slab ? SFL_PIPELINE_SLABS : (N.plane ? SFL_PIPELINE_PLANES : SFL_PIPELINE_LINES);
+    return N.slab ? SFL_PIPELINE_SLABS : SFL_PIPELINE_LINES;
 }
 
 // Tuned (pipeline, group) per transform, size and element type, for the
@@ -970,7 +970,6 @@ int sfl_ns_denoise(sfl_plan* plan, const void* x, void* y, const float* tau, voi
 
 static sfl::NSPlan& range_plan(sfl_plan* plan) {
     sfl::NSPlan& N = ns_of(plan, "item ranges");
-    if (N.plane) throw sfl::ArgError("item ranges need the slab or line pipeline");
     if (N.stream_mode != 0) throw sfl::ArgError("a streaming pass is in progress on this plan");
     return N;
 }

@@ -243,43 +243,6 @@ static std::vector<float> to_f32(const std::vector<double>& v) {
     return o;
 }
 
-// Builds the plane-major copies of the group tables and switches the plan to
-// the plane-major pipeline: (k1, k2, k3) -> k2 + n2 (k3 + n3 k1).
-void ns_use_planes(NSPlan& P) {
-    if (!ns_plane_supported(P.dims[0], P.dims[1], P.dims[2]))
-        throw ArgError("the plane-major pipeline does not support size " + std::to_string(P.dims[0]) + "x" +
-                       std::to_string(P.dims[1]) + "x" + std::to_string(P.dims[2]));
-    if (!P.Gp.p) {
-        // permute the float32 tables the plan already holds (designed on the device)
-        const int h1 = P.h1, n2 = P.dims[1], n3 = P.dims[2];
-        auto permute_all = [&](const DevMem& src, std::vector<float>& dst) {
-            const size_t n = src.p ? src.bytes / sizeof(float) / (size_t)P.H * (size_t)P.H : 0;
-            std::vector<float> g(n);
-            if (n) cuda_check(cudaMemcpy(g.data(), src.p, n * sizeof(float), cudaMemcpyDeviceToHost), "table readback");
-            dst.resize(n);
-            for (size_t base = 0; base < n; base += (size_t)P.H)
-                for (int k3 = 0; k3 < n3; ++k3)
-                    for (int k2 = 0; k2 < n2; ++k2)
-                        for (int k1 = 0; k1 < h1; ++k1)
-                            dst[base + k2 + (size_t)n2 * (k3 + (size_t)n3 * k1)] =
-                                g[base + k1 + (size_t)h1 * (k2 + (size_t)n2 * k3)];
-        };
-        std::vector<float> Gp, Blp;
-        permute_all(P.G, Gp);
-        if (!P.p.tight) permute_all(P.Bl, Blp);
-        upload(P.Gp, Gp);
-        upload(P.Blp, Blp);
-        P.tbp = P.tb;
-        P.tbp.G = P.Gp.as<float>();
-        P.tbp.Bl = P.Blp.as<float>();
-    }
-    P.plane = true;
-    if (P.slab) {
-        P.slab = false;
-        ns_alloc_scratch(P);
-    }
-}
-
 // With ndfb, the standalone directional bank of one level count
 // (src/directional/ndfb.jl:91-104; HourglassFB at level 0): the same cascade
 // with the hourglass masks alone as group factors, no pyramid and no lowpass.
@@ -766,7 +729,6 @@ ZMap ns_subband_map(const NSPlan& P, int i0, int es) {
 }
 
 void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks) {
-    if (P.plane) return ns_plane_analyze(P, x, c, st, synth_masks);
     if (P.slab) return ns_slab_analyze(P, x, c, st, synth_masks);
     const int es = P.nch;
     float2* X = P.X.as<float2>();
@@ -781,7 +743,6 @@ void ns_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_m
 }
 
 void ns_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks) {
-    if (P.plane) return ns_plane_synthesize(P, c, x, st, analysis_masks);
     if (P.slab) return ns_slab_synthesize(P, c, x, st, analysis_masks);
     const int es = P.nch;
     float2* A = P.acc.as<float2>();
@@ -819,13 +780,9 @@ void ns_selftest_wait(NSPlan& P, cudaStream_t st) {
 // ── streaming ────────────────────────────────────────────────────────────────
 
 void ns_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st) {
-    if (P.plane) {
-        ns_plane_stream_analyze_begin(P, x, st);
-    } else {
-        for (int ch = 0; ch < P.nch; ++ch)
-            ns_forward_spectrum(P, reinterpret_cast<const float*>(x) + ch, P.nch,
-                                P.X.as<float2>() + ch * ns_spec_elems(P), st);
-    }
+    for (int ch = 0; ch < P.nch; ++ch)
+        ns_forward_spectrum(P, reinterpret_cast<const float*>(x) + ch, P.nch, P.X.as<float2>() + ch * ns_spec_elems(P),
+                            st);
     P.stream_mode = 1;
     P.stream_pos = 0;
 }
@@ -837,13 +794,9 @@ int ns_stream_analyze_next(NSPlan& P, void* band, int* index, cudaStream_t st) {
         return SFL_DONE;
     }
     const NSItem& it = P.items_host[P.stream_pos];
-    if (P.plane) {
-        ns_plane_stream_analyze_one(P, P.stream_pos, band, st);
-    } else {
-        for (int ch = 0; ch < P.nch; ++ch)
-            ns_analyze_range(P, P.X.as<float2>() + ch * ns_spec_elems(P), reinterpret_cast<float*>(band) + ch, ZMap{},
-                             P.nch, P.stream_pos, 1, false, st);
-    }
+    for (int ch = 0; ch < P.nch; ++ch)
+        ns_analyze_range(P, P.X.as<float2>() + ch * ns_spec_elems(P), reinterpret_cast<float*>(band) + ch, ZMap{},
+                         P.nch, P.stream_pos, 1, false, st);
     *index = it.s;
     P.stream_pos += 1;
     return SFL_OK;
@@ -864,9 +817,7 @@ int ns_stream_synth_next_index(NSPlan& P, int* index) {
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
     if (P.stream_mode != 2) throw StateError("no streaming synthesis is open on this plan");
     if (P.stream_pos >= P.S) throw StateError("every subband has already been pushed");
-    if (P.plane) {
-        ns_plane_stream_synth_push(P, P.stream_pos, band, st);
-    } else {
+    {
         const long long E = ns_spec_elems(P);
         if (P.stream_pos == 0) {
             for (int ch = 0; ch < P.nch; ++ch) ns_acc_clear(P, P.acc.as<float2>() + ch * E, ns_comp_grid(P, ch), st);
@@ -895,13 +846,8 @@ void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st) {
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st) {
     if (P.stream_mode != 2 || P.stream_pos != P.S)
         throw StateError("streaming synthesis ended before every subband was pushed");
-    if (P.plane) {
-        ns_plane_stream_synth_end(P, x, st);
-    } else {
-        for (int ch = 0; ch < P.nch; ++ch)
-            ns_inverse_spectrum(P, P.acc.as<float2>() + ch * ns_spec_elems(P), reinterpret_cast<float*>(x) + ch, P.nch,
-                                st);
-    }
+    for (int ch = 0; ch < P.nch; ++ch)
+        ns_inverse_spectrum(P, P.acc.as<float2>() + ch * ns_spec_elems(P), reinterpret_cast<float*>(x) + ch, P.nch, st);
     P.stream_mode = 0;
 }
 

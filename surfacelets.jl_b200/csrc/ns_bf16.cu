@@ -73,7 +73,6 @@ __global__ void bf16_to_band_kernel(const __nv_bfloat16* __restrict__ in, const 
 }
 
 void need_bf16_path(const NSPlan& P) {
-    if (P.plane) throw ArgError("bfloat16 coefficients need the slab or line pipeline");
     if (P.nch != 1) throw ArgError("bfloat16 coefficients are for Float32 volumes");
 }
 

@@ -28,7 +28,6 @@ __global__ void soft_threshold_kernel(float* band, long long n, const float* __r
 }  // namespace
 
 void ns_denoise(NSPlan& P, const float* x, float* y, const float* tau, cudaStream_t st) {
-    if (P.plane) throw ArgError("the denoiser needs the slab or line pipeline");
     if (P.nch != 1) throw ArgError("the denoiser is for Float32 volumes");
     float2* X = P.X.as<float2>();
     float2* A = P.acc.as<float2>();

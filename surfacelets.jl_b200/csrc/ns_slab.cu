@@ -1167,7 +1167,6 @@ void ns_use_slabs(NSPlan& P) {
     if (!ns_slab_supported(P.dims[0], P.dims[1], P.dims[2]))
         throw ArgError("the slab pipeline does not support size " + std::to_string(P.dims[0]) + "x" +
                        std::to_string(P.dims[1]) + "x" + std::to_string(P.dims[2]));
-    P.plane = false;
     P.slab = true;
     ns_alloc_scratch(P);
 }

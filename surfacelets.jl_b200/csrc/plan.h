@@ -131,10 +131,6 @@ struct NSPlan {
     DevMem items;
     DevMem G, Bl, vec, planes;
     NSMaskTables tb;
-    // plane-major pipeline (sizes with pencil and plane kernels)
-    bool plane = false;
-    DevMem Gp, Blp;         // G and Bl in plane-major order
-    NSMaskTables tbp;
     HostWord status;        // status word of bounded waits (0 = fine), written by the kernels
     // slab pipeline (spectra with the axis-1 pitch padded to P1)
     bool slab = false;
@@ -182,9 +178,6 @@ void ns_stream_synth_begin(NSPlan& P, cudaStream_t st);
 int ns_stream_synth_next_index(NSPlan& P, int* index);
 void ns_stream_synth_push(NSPlan& P, const void* band, cudaStream_t st);
 void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
-// Plane-major pipeline (ns_plane.cu).
-bool ns_plane_supported(int n1, int n2, int n3);
-void ns_use_planes(NSPlan& P);
 // Group tables G, level bandpasses Bl and the per-table support boxes,
 // designed in float64 on the device (ns_design.cu).
 void ns_design_tables_device(NSPlan& P);
@@ -252,12 +245,6 @@ ZMap ns_subband_map(const NSPlan& P, int i0, int es);
 // bfloat16 coefficients with a float32 scale per subband (ns_bf16.cu).
 void ns_analyze_bf16(NSPlan& P, const float* x, void* c, float* scales, cudaStream_t st);
 void ns_synthesize_bf16(NSPlan& P, const void* c, const float* scales, float* x, cudaStream_t st);
-void ns_plane_analyze(NSPlan& P, const void* x, void* c, cudaStream_t st, bool synth_masks);
-void ns_plane_synthesize(NSPlan& P, const void* c, void* x, cudaStream_t st, bool analysis_masks);
-void ns_plane_stream_analyze_begin(NSPlan& P, const void* x, cudaStream_t st);
-void ns_plane_stream_analyze_one(NSPlan& P, int pos, void* band, cudaStream_t st);
-void ns_plane_stream_synth_push(NSPlan& P, int pos, const void* band, cudaStream_t st);
-void ns_plane_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
 // One analysis subband with static scratch (noalloc.cu).
 void ns_analyze_subband_static(NSPlan& P, const void* x, void* band, int index, cudaStream_t st);
 

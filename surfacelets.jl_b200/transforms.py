@@ -447,7 +447,8 @@ class Workspace:
 
     def set_pipeline(self, name):
         """NSSurfacelet kernel pipeline: "slabs" (the default where the size
-        allows), "lines" or "planes"."""
+        allows) or "lines" ("planes", the retired plane-major pipeline, is
+        refused by the library)."""
         if name not in self.PIPELINES:
             raise ArgumentError(f"unknown pipeline {name!r}; expected one of {sorted(self.PIPELINES)}")
         check(lib.sfl_plan_set_pipeline(self._h, self.PIPELINES[name]))

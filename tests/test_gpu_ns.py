@@ -41,8 +41,7 @@ CASES = [
     ((128, 128, 64), dict(scales=2, direction_levels=[2, 2], bernstein_order=8, tight=False)),
     ((64, 96, 32), dict(scales=3, direction_levels=[1, 2, 2], bernstein_order=8)),
 ]
-PIPELINE_CASES = ([(d, k, "lines") for d, k in CASES] + [(d, k, "planes") for d, k in CASES[-4:-1]]
-                  + [(d, k, "slabs") for d, k in CASES[-4:]])
+PIPELINE_CASES = [(d, k, "lines") for d, k in CASES] + [(d, k, "slabs") for d, k in CASES[-4:]]
 
 
 @pytest.mark.parametrize("dims,kw,pipeline", PIPELINE_CASES)
@@ -144,7 +143,7 @@ def test_streaming_matches_materialized(sfl):
 
 
 @pytest.mark.parametrize("dims,pipeline", [((64, 64, 64), "slabs"), ((64, 64, 64), "lines"),
-                                           ((64, 64, 64), "planes"), ((16, 16, 16), "lines")])
+                                           ((16, 16, 16), "lines")])
 @pytest.mark.parametrize("dtype", ["float32", "complex64"])
 def test_streaming_equals_materialized_bit_for_bit(sfl, dims, pipeline, dtype):
     # test/items/test_ns_surfacelet.jl:79-106, 108-138
@@ -212,7 +211,7 @@ def test_group_size_does_not_change_results(sfl, dims, pipeline):
 
 def test_pipeline_selection_is_validated(sfl):
     ws = sfl.make_workspace(sfl.NSSurfacelet(scales=1, direction_levels=[1], bernstein_order=4), "float32", (12, 10, 8))
-    with pytest.raises(sfl.ArgumentError, match="plane-major pipeline does not support"):
+    with pytest.raises(sfl.ArgumentError, match="plane-major pipeline was retired"):
         ws.set_pipeline("planes")
     with pytest.raises(sfl.ArgumentError, match="slab pipeline does not support"):
         ws.set_pipeline("slabs")
