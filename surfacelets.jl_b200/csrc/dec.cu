@@ -20,6 +20,7 @@
 #include "passes.cuh"
 #include "plan.h"
 #include "regpass.cuh"
+#include "slab_core.cuh"
 
 namespace sfl {
 
@@ -199,7 +200,10 @@ __global__ void irc_stage_kernel(float2* S, int h0, int h1, int h2, int K, int m
 
 // Every IRC stage of hourglass K on one plane k_K of S_K (the plane over the
 // two transverse axes), held in shared memory: one HBM round trip for the
-// whole cascade instead of one per stage.  The analysis form applies the
+// whole cascade instead of one per stage.  Where both block lengths have a
+// register line FFT, the block FFTs along the two transverse axes run in the
+// same pass (after the stages in the analysis, before them in the
+// synthesis): every block lies inside one plane.  The analysis form applies the
 // hourglass mask on load (S_K = X[half_K] V_K s, as hg_mask_kernel) and runs
 // the stages in order; the synthesis form runs them in reverse with the
 // synthesis filters.  Per stage the same butterfly, in the same order of
@@ -224,11 +228,89 @@ struct IrcPlaneJob {
     const float* V;   // analysis: the hourglass mask V_K and the subband scale s
     float s;
     IrcPlaneStages sg;
+    // the block FFTs along the two transverse axes, fused: segment lengths (0: run separately) and the
+    // twiddle tables w_bs^k of those lengths
+    int bs1, bs2;
+    const float2* tw1;
+    const float2* tw2;
 };
 struct IrcPlaneJobs {
     int n;
     IrcPlaneJob job[3];
 };
+
+// Plane pitch: the first transverse length rounded to 2 mod 4, so that lines
+// along either axis of the plane are free of bank conflicts.
+__host__ __device__ inline int irc_plane_pitch(int a1) { return a1 % 4 == 0 ? a1 + 2 : a1; }
+
+// Block FFT lengths the plane pass runs itself (register line FFTs of at most
+// 16 values a thread, within the 64 registers of a 1024-thread CTA).
+__host__ __device__ inline bool irc_plane_block_len(int n) { return n == 16 || n == 32 || n == 64 || n == 128; }
+
+// The segmented FFTs of the plane along one transverse axis: segments of N
+// points (the block length), unnormalized, inverse or forward.  Lines of a
+// warp sit on consecutive rows (along the first axis) or consecutive columns
+// (along the second), so their slots fall on distinct banks.
+template <int N, bool INV>
+__device__ void irc_plane_seg_fft(float2* pl, int ap, int a1, int a2, bool along1, const float2* tw2s) {
+    using LN = SlabLine<N>;
+    constexpr int N1 = LN::N1, N2 = LN::N2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int p = lane & (N2 - 1), sl = lane / N2;
+    const int nseg = (along1 ? a1 : a2) / N;
+    const int nl = (along1 ? a2 : a1) * nseg;
+    for (int b0 = 0; b0 < nl; b0 += nwarps * LN::LPW) {
+        if (b0 + warp * LN::LPW >= nl) continue;   // warp-uniform
+        const int line = b0 + warp * LN::LPW + sl;
+        const bool valid = line < nl;
+        const int li = valid ? line : 0;
+        float2* base;
+        int stride;
+        if (along1) {
+            const int o2 = li % a2, seg = li / a2;
+            base = pl + (long long)o2 * ap + seg * N;
+            stride = 1;
+        } else {
+            const int o1 = li % a1, seg = li / a1;
+            base = pl + o1 + (long long)seg * N * ap;
+            stride = ap;
+        }
+        float2 v[N1];
+#pragma unroll
+        for (int r = 0; r < N1; ++r) v[r] = valid ? base[stride * (p + N2 * r)] : make_float2(0.f, 0.f);
+        warp_line_fft_rs<N, INV>(v, p, valid, tw2s, base, stride);
+        if (valid) {
+#pragma unroll
+            for (int j = 0; j < LN::M; ++j)
+#pragma unroll
+                for (int k = 0; k < N2; ++k) base[stride * ((p + N2 * j) + N1 * k)] = v[j * N2 + k];
+        }
+    }
+}
+
+template <bool INV>
+__device__ void irc_plane_block_ffts(float2* pl, int ap, int a1, int a2, int bs, bool along1, const float2* tw2s) {
+    switch (bs) {
+        case 16: irc_plane_seg_fft<16, INV>(pl, ap, a1, a2, along1, tw2s); break;
+        case 32: irc_plane_seg_fft<32, INV>(pl, ap, a1, a2, along1, tw2s); break;
+        case 64: irc_plane_seg_fft<64, INV>(pl, ap, a1, a2, along1, tw2s); break;
+        case 128: irc_plane_seg_fft<128, INV>(pl, ap, a1, a2, along1, tw2s); break;
+    }
+}
+
+template <int N>
+__device__ void irc_plane_twiddles(float2* tw2s, const float2* tw) {
+    load_slab_twiddles<N>(tw2s, tw);
+}
+
+__device__ void irc_plane_load_twiddles(float2* tw2s, const float2* tw, int bs) {
+    switch (bs) {
+        case 16: irc_plane_twiddles<16>(tw2s, tw); break;
+        case 32: irc_plane_twiddles<32>(tw2s, tw); break;
+        case 64: irc_plane_twiddles<64>(tw2s, tw); break;
+        case 128: irc_plane_twiddles<128>(tw2s, tw); break;
+    }
+}
 
 template <bool SYNTH>
 __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJobs jobs, const float2* __restrict__ X,
@@ -254,6 +336,14 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJob
     const long long base = (long long)kK * sK;
     const long long xbase = (long long)kK * xK;
     const int tot = a1 * a2;
+    const int ap = irc_plane_pitch(a1);                  // the plane's row pitch in shared memory
+    float2* cf = pl + (long long)ap * a2;                // a stage's two filter rows
+    float2* tws = cf + 2 * (a1 > a2 ? a1 : a2);          // block-FFT twiddles: bs1 then bs2 entries
+    const bool fused = jb.bs1 > 0 && jb.bs2 > 0;
+    if (fused) {
+        irc_plane_load_twiddles(tws, jb.tw1, jb.bs1);
+        irc_plane_load_twiddles(tws + jb.bs1, jb.tw2, jb.bs2);
+    }
     // kIrcPlaneBatch independent loads in flight per thread (one CTA an SM holds the plane)
     for (int q0 = threadIdx.x; q0 < tot; q0 += kIrcPlaneBatch * blockDim.x) {
         float2 v[kIrcPlaneBatch];
@@ -274,10 +364,17 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJob
 #pragma unroll
         for (int u = 0; u < kIrcPlaneBatch; ++u) {
             const int q = q0 + u * blockDim.x;
-            if (q < tot) pl[q] = v[u];
+            if (q < tot) pl[(q % a1) + ap * (q / a1)] = v[u];
         }
     }
     __syncthreads();
+    if (SYNTH && fused) {
+        // subband -> block: the forward block FFTs along both transverse axes, then the stages in reverse
+        irc_plane_block_ffts<false>(pl, ap, a1, a2, jb.bs1, true, tws);
+        __syncthreads();
+        irc_plane_block_ffts<false>(pl, ap, a1, a2, jb.bs2, false, tws + jb.bs1);
+        __syncthreads();
+    }
     for (int t = 0; t < sg.n; ++t) {
         const int u = SYNTH ? sg.n - 1 - t : t;
         const int b = sg.b[u];
@@ -286,7 +383,6 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJob
         const int npairs = half * (first ? a2 : a1);
         // the stage's filter row at k_K (over the stage's axis) into shared memory
         const int am = first ? a1 : a2;
-        float2* cf = pl + tot;
         for (int i = threadIdx.x; i < am; i += blockDim.x) {
             cf[i] = sg.f0[u][kK + (long long)nKh * i];
             cf[am + i] = sg.f1[u][kK + (long long)nKh * i];
@@ -304,8 +400,8 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJob
                 pq = q / a1;
             }
             const int cA = (pq / b) * 2 * b + (pq % b), cB = cA + b;
-            const int qA = first ? cA + a1 * o : o + a1 * cA;
-            const int qB = first ? cB + a1 * o : o + a1 * cB;
+            const int qA = first ? cA + ap * o : o + ap * cA;
+            const int qB = first ? cB + ap * o : o + ap * cB;
             const float2 A = pl[qA], Bv = pl[qB];
             const float2 f0A = cf[cA], f0B = cf[cB], f1A = cf[am + cA], f1B = cf[am + cB];
             float2 nA, nB;
@@ -321,9 +417,16 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJob
         }
         __syncthreads();
     }
+    if (!SYNTH && fused) {
+        // block -> subband, first half: the inverse block FFTs along both transverse axes
+        irc_plane_block_ffts<true>(pl, ap, a1, a2, jb.bs1, true, tws);
+        __syncthreads();
+        irc_plane_block_ffts<true>(pl, ap, a1, a2, jb.bs2, false, tws + jb.bs1);
+        __syncthreads();
+    }
     for (int q = threadIdx.x; q < tot; q += blockDim.x) {
         const int i1 = q % a1, i2 = q / a1;
-        S[base + i1 * s1 + i2 * s2] = pl[q];
+        S[base + i1 * s1 + i2 * s2] = pl[i1 + ap * i2];
     }
 }
 
@@ -762,7 +865,7 @@ struct RStoreCJobs {
 // The block FFTs of every hourglass of level L along both transverse axes,
 // grouped into one launch per (block length, line layout); lengths without a
 // register pass run one segmented pass per spectrum and axis.
-void block_fft_level(DecPlan& D, DecLevelDev& L, bool inv, cudaStream_t st) {
+void block_fft_level(DecPlan& D, DecLevelDev& L, bool inv, const bool skip[3], cudaStream_t st) {
     struct Item {
         int K, m, bl;
         bool tf;
@@ -772,7 +875,7 @@ void block_fft_level(DecPlan& D, DecLevelDev& L, bool inv, cudaStream_t st) {
     int ni = 0;
     for (int K = 0; K < 3; ++K)
         for (int m = 0; m < 3; ++m)
-            if (m != K) items[ni++] = Item{K, m, L.bsize[K][m], m != 0, false};
+            if (m != K && !skip[K]) items[ni++] = Item{K, m, L.bsize[K][m], m != 0, false};
     for (int a = 0; a < ni; ++a) {
         if (items[a].done) continue;
         LineJobs jobs;
@@ -889,7 +992,15 @@ void pyr_merge(DecPlan& D, int j, cudaStream_t st, bool adjoint = false) {
 size_t irc_plane_smem(const DecLevelDev& L, int K) {
     const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
     const int a1 = L.hd[K][m1], a2 = L.hd[K][m2];
-    return sizeof(float2) * ((size_t)a1 * a2 + 2 * (size_t)std::max(a1, a2));   // the plane + a stage's filter row
+    // the padded plane, a stage's two filter rows and the two block lengths' twiddles
+    return sizeof(float2) * ((size_t)irc_plane_pitch(a1) * a2 + 2 * (size_t)std::max(a1, a2) + (size_t)a1 + a2);
+}
+
+// Whether the plane pass of hourglass K also runs its block FFTs (both block
+// lengths with a register line FFT).
+bool irc_plane_fuses_blocks(const DecLevelDev& L, int K) {
+    const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
+    return irc_plane_block_len(L.bsize[K][m1]) && irc_plane_block_len(L.bsize[K][m2]);
 }
 
 bool irc_plane_fits(const DecLevelDev& L, int K) {
@@ -924,7 +1035,7 @@ void irc_plane_configure(size_t smem) {
 // fits (analysis: with the mask on load from the level spectrum X; synthesis:
 // hourglasses without stages have nothing to do).
 template <bool SYNTH>
-void irc_plane_launch(DecPlan& D, DecLevelDev& L, const float2* X, cudaStream_t st) {
+void irc_plane_launch(DecPlan& D, DecLevelDev& L, const float2* X, const bool fuse[3], cudaStream_t st) {
     IrcPlaneJobs jobs{};
     size_t smem = 0;
     int blocks = 0;
@@ -940,6 +1051,13 @@ void irc_plane_launch(DecPlan& D, DecLevelDev& L, const float2* X, cudaStream_t 
         for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
         jb.s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
         jb.sg = irc_plane_stages(L, K, SYNTH);
+        if (fuse[K]) {
+            const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
+            jb.bs1 = L.bsize[K][m1];
+            jb.bs2 = L.bsize[K][m2];
+            jb.tw1 = get_fft(D.ffts, jb.bs1)->sh.tw;
+            jb.tw2 = get_fft(D.ffts, jb.bs2)->sh.tw;
+        }
         blocks += L.hd[K][K];
         smem = std::max(smem, irc_plane_smem(L, K));
     }
@@ -954,8 +1072,11 @@ void irc_plane_launch(DecPlan& D, DecLevelDev& L, const float2* X, cudaStream_t 
 void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
     const float2* X = D.spectra[j]->as<float2>();
-    // mask and every stage of each hourglass whose plane fits: one pass over the k_K planes of all three
-    irc_plane_launch<false>(D, L, X, st);
+    // mask, every stage and (where both lengths allow) the block FFTs of each hourglass whose plane fits:
+    // one pass over the k_K planes of all three
+    bool fuse[3];
+    for (int K = 0; K < 3; ++K) fuse[K] = irc_plane_fits(L, K) && irc_plane_fuses_blocks(L, K);
+    irc_plane_launch<false>(D, L, X, fuse, st);
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
         float2* S = D.S[K].as<float2>();
@@ -981,8 +1102,8 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
             }
         }
     }
-    // the block FFTs of all three hourglasses, grouped by length and layout
-    block_fft_level(D, L, true, st);
+    // the block FFTs of the other hourglasses, grouped by length and layout
+    block_fft_level(D, L, true, fuse, st);
     for (int K = 0; K < 3; ++K) {
         float2* S = D.S[K].as<float2>();
         Lines gk = k_lines(L, K);
@@ -1015,8 +1136,11 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
             launch_pass(ld, sto, f->sh, pairs, 1, false, st, "dec_r2c_blocks");
         }
     }
-    // the block FFTs of all three hourglasses, grouped by length and layout
-    block_fft_level(D, L, false, st);
+    // the block FFTs of the hourglasses whose plane pass does not run them, grouped by length and layout
+    bool fuse[3];
+    for (int K = 0; K < 3; ++K)
+        fuse[K] = irc_plane_fits(L, K) && !L.stages[K].empty() && irc_plane_fuses_blocks(L, K);
+    block_fft_level(D, L, false, fuse, st);
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
         float2* S = D.S[K].as<float2>();
@@ -1038,7 +1162,7 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
         ha.V[K] = L.V[K].as<float>();
     }
     // every stage, in reverse, of each hourglass whose plane fits: one pass over the k_K planes of all three
-    irc_plane_launch<true>(D, L, nullptr, st);
+    irc_plane_launch<true>(D, L, nullptr, fuse, st);
     long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
     {
         int tok = prof_begin("dec_herm_sum", st);

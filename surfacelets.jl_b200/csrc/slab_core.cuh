@@ -99,6 +99,43 @@ __device__ __forceinline__ void warp_line_fft(float2 (&v)[LinePlan<N>::N1], int 
     __syncwarp();   // slots are free again
 }
 
+// The same line FFT over slots base[stride t] with a run-time stride (a plane
+// of another pitch); conflict-free for stride = 1 or 2 mod 4.
+template <int N, bool INV>
+__device__ __forceinline__ void warp_line_fft_rs(float2 (&v)[LinePlan<N>::N1], int p, bool valid,
+                                                 const float2* __restrict__ tw2, float2* base, int stride) {
+    using L = SlabLine<N>;
+    constexpr int N1 = L::N1, N2 = L::N2;
+    RegDft<N1, INV>::run(v);
+#pragma unroll
+    for (int m = 1; m < N1; ++m) {
+        float2 w = tw2[m * N2 + p];
+        if (INV) w.y = -w.y;
+        v[m] = c_mul(v[m], w);
+    }
+    int xo[N2];
+#pragma unroll
+    for (int c = 0; c < N2; ++c) xo[c] = stride * (p ^ c);
+    __syncwarp();
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < N1; ++m) base[xo[m & (N2 - 1)] + stride * N2 * m] = v[m];
+    }
+    __syncwarp();
+    const float2* rb = base + stride * N2 * p;
+#pragma unroll
+    for (int j = 0; j < L::M; ++j) {
+        float2 w[N2];
+#pragma unroll
+        for (int pp = 0; pp < N2; ++pp)
+            w[pp] = valid ? rb[xo[pp] + stride * N2 * N2 * j] : make_float2(0.f, 0.f);
+        RegDft<N2, INV>::run(w);
+#pragma unroll
+        for (int k = 0; k < N2; ++k) v[j * N2 + k] = w[k];
+    }
+    __syncwarp();
+}
+
 // Lane layout of the column-pair phases: p fastest, then the line; with four
 // lines a warp, the two lines of a half warp are two apart so that their
 // columns fall on disjoint banks (P1 = 2 mod 4).
