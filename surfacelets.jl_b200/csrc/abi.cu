@@ -1093,6 +1093,21 @@ int sfl_ns_inverse_spectrum(sfl_plan* plan, void* A, void* x, void* stream) {
 
 // ── batches: one CUDA graph over many transforms ─────────────────────────────
 
+// Estimated work of one batch entry: the volume's voxels times (1 + coefficients a voxel); a volume copy
+// counts as its voxels.
+static double entry_work(const sfl_plan* plan, int op) {
+    const sfl::Plan& P = plan->impl;
+    double vox = 1, coef = 0;
+    if (P.kind == SFL_KIND_NS) {
+        vox = (double)P.ns->N;
+        coef = (double)P.ns->S;
+    } else {
+        for (int d = 0; d < 3; ++d) vox *= sfl::dec_design(*P.dec).dims[d];
+        coef = (double)sfl::dec_ncoeffs(*P.dec) / vox;
+    }
+    return op == SFL_OP_COPY_VOLUME ? vox : vox * (1 + coef);
+}
+
 int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, const void* const* inputs,
                      void* const* outputs, sfl_batch** out) {
     return guarded([&] {
@@ -1104,9 +1119,13 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, cons
         *out = nullptr;
         if (n < 1) throw sfl::ArgError("a batch needs at least one transform, got " + std::to_string(n));
         const int dev = (need(plans[0], "plans[0]"), plans[0]->impl.device);
-        // distinct plans run on up to kBranches concurrent branches; one plan always on the same branch
-        constexpr int kBranches = 8;
+        // distinct plans run on up to kBranches concurrent branches; one plan always on the same branch, the
+        // plans dealt out largest first to the branch with the least work so far (longest-processing-time
+        // order), the work of an entry estimated as voxels x (1 + coefficients per voxel)
+        constexpr int kBranches = 16;
         std::vector<const sfl_plan*> distinct;
+        std::vector<double> work;
+        std::vector<int> plan_of(n);
         std::vector<int> branch(n);
         for (int i = 0; i < n; ++i) {
             need(plans[i], "plans[i]");
@@ -1124,9 +1143,24 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, cons
             auto it = std::find(distinct.begin(), distinct.end(), plans[i]);
             if (it == distinct.end()) {
                 distinct.push_back(plans[i]);
+                work.push_back(0.0);
                 it = distinct.end() - 1;
             }
-            branch[i] = (int)(it - distinct.begin()) % kBranches;
+            plan_of[i] = (int)(it - distinct.begin());
+            work[plan_of[i]] += entry_work(plans[i], ops[i]);
+        }
+        {
+            std::vector<int> order(distinct.size());
+            for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+            std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+            std::vector<double> load(kBranches, 0.0);
+            std::vector<int> br(distinct.size());
+            for (int k : order) {
+                const int to = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+                br[k] = to;
+                load[to] += work[k];
+            }
+            for (int i = 0; i < n; ++i) branch[i] = br[plan_of[i]];
         }
         std::unique_ptr<sfl_batch> b(new sfl_batch());
         b->device = dev;

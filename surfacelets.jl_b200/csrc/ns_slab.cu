@@ -424,6 +424,8 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
         const int ch = u / per, ur = u - ch * per;
         const int z = ur / a.n3, s3 = ur - z * a.n3;
         const float2* src = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
+        // the output slab (its offset may come from the item table: loaded ahead of the phases)
+        float* out = a.vol + ch + a.vz.off(z) + (long long)s3 * PLANE * ES;
         // 1. the box of the slab into shared memory
         slab_bulk_load<NB, P1>(S, src, nk1, nk2, b2, bar, phase, a.status);
         // 2. inverse FFT along axis 2 of the rows k1 < nk1; columns outside the box are zero
@@ -455,7 +457,6 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
         {
             const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
             constexpr int npairs = NB / 2;
-            float* out = a.vol + ch + a.vz.off(z) + (long long)s3 * PLANE * ES;
             for (int base = 0; base < npairs; base += LA::LPR) {
                 if (base + warp * LA::LPW >= npairs) continue;   // warp-uniform
                 const int l = base + warp * LA::LPW + s;
