@@ -90,6 +90,7 @@ SIGNATURES = {
     "sfl_plan_autotune": (C.c_int, [P, P, P, P]),
     "sfl_plan_status": (C.c_int, [P, C.POINTER(C.c_int32), C.c_int32]),
     "sfl_plan_selftest_wait": (C.c_int, [P, P]),
+    "sfl_plan_tile": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int32)]),
     "sfl_analyze": (C.c_int, [P, P, P, P]),
     "sfl_synthesize": (C.c_int, [P, P, P, P]),
     "sfl_adjoint_analyze": (C.c_int, [P, P, P, P]),

@@ -146,8 +146,9 @@ void check_timeout(const sfl_plan* plan) {
     }
 }
 
-// Pipeline and group of an NS plan (the two knobs of the tuner).
-void ns_apply(sfl::NSPlan& N, int pipeline, int group) {
+// Pipeline, group and axis-3 tile of an NS plan (the knobs of the tuner).
+void ns_apply(sfl::NSPlan& N, int pipeline, int group, int ipc = -1) {
+    if (ipc >= 0) N.ipc = ipc;
     cudaDeviceSynchronize();
     if (pipeline == SFL_PIPELINE_LINES) {
         if (N.slab) {
@@ -175,7 +176,10 @@ int ns_pipeline_of(const sfl::NSPlan& N) {
 // Tuned (pipeline, group) per transform, size and element type, for the
 // lifetime of the process; plans created later with the same key start tuned.
 std::mutex g_tuned_mu;
-std::map<std::string, std::pair<int, int>> g_tuned;
+struct Tuning {
+    int pipeline, group, ipc;
+};
+std::map<std::string, Tuning> g_tuned;
 
 std::string tune_key(const sfl::NSPlan& N, int dtype) {
     std::string k = (N.ndfb ? "ndfb" : "ns") + std::string(":");
@@ -189,14 +193,14 @@ std::string tune_key(const sfl::NSPlan& N, int dtype) {
 
 void apply_tuned(sfl_plan* plan) {
     sfl::NSPlan& N = *plan->impl.ns;
-    std::pair<int, int> t;
+    Tuning t;
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
         auto it = g_tuned.find(tune_key(N, plan->impl.dtype));
         if (it == g_tuned.end()) return;
         t = it->second;
     }
-    ns_apply(N, t.first, t.second);
+    ns_apply(N, t.pipeline, t.group, t.ipc);
 }
 
 // One transform of a plan (the four operators of the C ABI).
@@ -584,29 +588,49 @@ int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream) {
         check_aligned(c, plan->impl.dtype, "c");
         on_device(plan, [&] {
             cudaStream_t st = as_stream(stream);
-            std::vector<int> pipes;
-            if (sfl::ns_slab_supported(N.dims[0], N.dims[1], N.dims[2])) pipes.push_back(SFL_PIPELINE_SLABS);
-            pipes.push_back(SFL_PIPELINE_LINES);
             cudaEvent_t e0, e1;
             sfl::cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
             sfl::cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+            // analysis, then synthesis of its coefficients into a scratch volume, twice after a warm-up
+            sfl::DevMem y;
+            y.alloc(sizeof(float) * (size_t)N.N * N.nch);
+            auto time_it = [&](int pipe, int g, int ipc) {
+                ns_apply(N, pipe, g, ipc);
+                sfl::ns_analyze(N, x, c, st, false);   // warm-up
+                sfl::cuda_check(cudaEventRecord(e0, st), "cudaEventRecord");
+                for (int r = 0; r < 2; ++r) {
+                    sfl::ns_analyze(N, x, c, st, false);
+                    sfl::ns_synthesize(N, c, y.p, st, false);
+                }
+                sfl::cuda_check(cudaEventRecord(e1, st), "cudaEventRecord");
+                sfl::cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+                float ms = 0;
+                sfl::cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                return ms;
+            };
+            Tuning pick{ns_pipeline_of(N), N.group, N.ipc};
             float best = 1e30f;
-            std::pair<int, int> pick{ns_pipeline_of(N), N.group};
             try {
+                std::vector<int> pipes;
+                if (sfl::ns_slab_supported(N.dims[0], N.dims[1], N.dims[2])) pipes.push_back(SFL_PIPELINE_SLABS);
+                pipes.push_back(SFL_PIPELINE_LINES);
+                // pipeline x group at the default tile, then the slab tile (subbands a CTA of the axis-3
+                // analysis pass) for the best group
                 for (int pipe : pipes)
                     for (int g : {2, 4, 8}) {
                         if (g > N.S && g != 2) continue;
-                        ns_apply(N, pipe, g);
-                        sfl::ns_analyze(N, x, c, st, false);   // warm-up
-                        sfl::cuda_check(cudaEventRecord(e0, st), "cudaEventRecord");
-                        for (int r = 0; r < 2; ++r) sfl::ns_analyze(N, x, c, st, false);
-                        sfl::cuda_check(cudaEventRecord(e1, st), "cudaEventRecord");
-                        sfl::cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
-                        float ms = 0;
-                        sfl::cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                        const float ms = time_it(pipe, g, 0);
                         if (ms < best) {
                             best = ms;
-                            pick = {pipe, g};
+                            pick = {pipe, g, 0};
+                        }
+                    }
+                if (pick.pipeline == SFL_PIPELINE_SLABS)
+                    for (int ipc : {1, 2}) {
+                        const float ms = time_it(pick.pipeline, pick.group, ipc);
+                        if (ms < best) {
+                            best = ms;
+                            pick.ipc = ipc;
                         }
                     }
             } catch (...) {
@@ -616,7 +640,7 @@ int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream) {
             }
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
-            ns_apply(N, pick.first, pick.second);
+            ns_apply(N, pick.pipeline, pick.group, pick.ipc);
             std::lock_guard<std::mutex> lk(g_tuned_mu);
             g_tuned[tune_key(N, plan->impl.dtype)] = pick;
         });
@@ -707,6 +731,21 @@ int sfl_plan_selftest_wait(sfl_plan* plan, void* stream) {
     return guarded([&] {
         sfl::NSPlan& N = ns_of(plan, "the bounded-wait self-test");
         on_device(plan, [&] { sfl::ns_selftest_wait(N, as_stream(stream)); });
+        return SFL_OK;
+    });
+}
+
+int sfl_plan_tile(sfl_plan* plan, int32_t set, int32_t* ipc) {
+    return guarded([&] {
+        sfl::NSPlan& N = ns_of(plan, "the axis-3 tile");
+        need(ipc, "ipc");
+        if (set) {
+            if (*ipc != 0 && *ipc != 1 && *ipc != 2 && *ipc != 4)
+                throw sfl::ArgError("subbands a CTA must be 1, 2 or 4 (0: the default), got " + std::to_string(*ipc));
+            N.ipc = *ipc;
+        } else {
+            *ipc = N.ipc;
+        }
         return SFL_OK;
     });
 }

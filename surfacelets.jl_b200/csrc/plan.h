@@ -127,6 +127,7 @@ struct NSPlan {
     int nch = 1;          // 1 real, 2 complex
     bool ndfb = false;    // the standalone directional bank (no pyramid, no lowpass)
     int group = 8;
+    int ipc = 0;          // subbands a CTA of the slab axis-3 analysis pass takes (1, 2, 4; 0: 4, or SFL_MASK_IPC)
     std::vector<NSItem> items_host;   // streaming / item order: directional ascending, then lowpass
     DevMem items;
     DevMem G, Bl, vec, planes;

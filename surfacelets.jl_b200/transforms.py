@@ -432,9 +432,17 @@ class Workspace:
         names = {v: k for k, v in self.PIPELINES.items()}
         return names.get(pi.value), g.value
 
+    def tile(self, ipc=None):
+        """Subbands a CTA of the slab pipeline's axis-3 analysis pass takes
+        (1, 2 or 4; 0 = the default): read, or set when ipc is given."""
+        v = C.c_int32(0 if ipc is None else int(ipc))
+        check(lib.sfl_plan_tile(self._h, 0 if ipc is None else 1, C.byref(v)))
+        return v.value
+
     def autotune(self, x=None, stream=None):
-        """Time analysis under each pipeline and group size, keep the fastest and
-        remember it for later workspaces of the same transform, size and type.
+        """Time analysis + synthesis under each pipeline and group size (and the
+        slab pipeline's axis-3 tile), keep the fastest and remember it for later
+        workspaces of the same transform, size and type.
         x: a device volume to time on (random when omitted)."""
         if not isinstance(self.transform, NSSurfacelet):
             return self.tuning()

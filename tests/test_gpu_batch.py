@@ -168,3 +168,23 @@ def test_mixed_batch_as_one_graph(sfl):
         assert torch.equal(y, sfl.synthesize(ws, c0))
         assert float(torch.linalg.vector_norm(y - x) / torch.linalg.vector_norm(x)) <= 1e-5
     b.close()
+
+
+def test_axis3_tile_is_tunable_and_does_not_change_results(sfl):
+    """Subbands a CTA of the slab axis-3 analysis pass (the tile the autotuner
+    picks): 1, 2 and 4 give the same coefficients bit for bit."""
+    dims = (64, 64, 64)
+    t = sfl.NSSurfacelet(scales=3, direction_levels=[2, 2, 3])
+    ws = sfl.make_workspace(t, "float32", dims)
+    x = sfl.to_device(np.random.default_rng(12).standard_normal(dims).astype(np.float32))
+    assert ws.tile() == 0
+    ref = sfl.analyze(ws, x)
+    for ipc in (1, 2, 4):
+        assert ws.tile(ipc) == ipc and ws.tile() == ipc
+        assert torch.equal(sfl.analyze(ws, x), ref), ipc
+    with pytest.raises(sfl.ArgumentError, match="1, 2 or 4"):
+        ws.tile(3)
+    ws.tile(0)
+    ws.autotune(x)
+    assert ws.tile() in (0, 1, 2)
+    assert torch.equal(sfl.analyze(ws, x), ref) or ws.tuning()[0] == "lines"
