@@ -450,66 +450,6 @@ __device__ __forceinline__ void slab_rows_inverse(float2* S, int nk1, int b2, in
     }
 }
 
-// Forward FFT along axis 2 of the slab's rows k1 < nk1, in place.  When the
-// rows span every k1 (nk1 = NA/2 + 1), rows 0 and NA/2 are real (the R2C
-// along axis 1 leaves exact zeros in their imaginary parts): they share one
-// complex line W = row_0 + i row_NA/2, and the two transforms follow from
-// F = FFT(W) as (F[k] + conj F[-k]) / 2 and (F[k] - conj F[-k]) / 2i, read
-// through the line's slots in row 0, so the rows take one round fewer.
-template <int NA, int NB>
-__device__ __forceinline__ void slab_rows_forward(float2* S, int nk1, const float2* twB, int lane, int warp) {
-    using LB = SlabLine<NB>;
-    constexpr int P1 = slab_pitch_c(NA / 2 + 1);
-    const bool pack = nk1 == NA / 2 + 1;
-    const int nrows = pack ? nk1 - 1 : nk1;   // with pack, line 0 carries rows 0 and NA/2
-    const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
-    for (int base = 0; base < nrows; base += LB::LPR) {
-        if (base + warp * LB::LPW >= nrows) continue;   // warp-uniform
-        const int k1 = base + warp * LB::LPW + s;
-        const bool valid = k1 < nrows;
-        const bool two = pack && k1 == 0;
-        float2* row = S + (valid ? k1 : 0);
-        float2* row2 = S + NA / 2;
-        float2 v[LB::N1];
-#pragma unroll
-        for (int r = 0; r < LB::N1; ++r) {
-            float2 a = valid ? row[P1 * (p + LB::N2 * r)] : make_float2(0.f, 0.f);
-            if (two) a = make_float2(a.x, row2[P1 * (p + LB::N2 * r)].x);
-            v[r] = a;
-        }
-        warp_line_fft<NB, false, P1>(v, p, valid, twB, row);
-        if (valid) {
-#pragma unroll
-            for (int j = 0; j < LB::M; ++j)
-#pragma unroll
-                for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
-        }
-        if (pack && base == 0 && warp == 0) {   // warp-uniform: the warp holding line 0
-            __syncwarp();   // F of the packed line complete in row 0
-#pragma unroll
-            for (int j = 0; j < LB::M; ++j)
-#pragma unroll
-                for (int k = 0; k < LB::N2; ++k) {
-                    const int i = (p + LB::N2 * j) + LB::N1 * k;
-                    if (two) {
-                        const float2 zk = v[j * LB::N2 + k];
-                        const float2 zn = row[P1 * (i == 0 ? 0 : NB - i)];
-                        v[j * LB::N2 + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-                        row2[P1 * i] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
-                    }
-                }
-            __syncwarp();   // every lane has read F before row 0 is overwritten
-            if (two) {
-#pragma unroll
-                for (int j = 0; j < LB::M; ++j)
-#pragma unroll
-                    for (int k = 0; k < LB::N2; ++k)
-                        row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
-            }
-        }
-    }
-}
-
 // Analysis slab pass (inverse): spectra -> real volumes (element stride ES).
 // The exchange slots of a column pair are the pair's two columns read as one
 // run of 2 P1 >= NA values.
@@ -669,7 +609,25 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
         }
         __syncthreads();
         // 2. forward FFT along axis 2 of the rows k1 < nk1
-        slab_rows_forward<NA, NB>(S, nk1, twB, lane, warp);
+        {
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) v[r] = valid ? row[P1 * (p + LB::N2 * r)] : make_float2(0.f, 0.f);
+                warp_line_fft<NB, false, P1>(v, p, valid, twB, row);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
         __syncthreads();
         // 3. the box of the slab out to the spectrum
         float2* dst = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
@@ -790,8 +748,25 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_shrink_kernel(Slab
             }
         }
         __syncthreads();
-        // forward FFT along axis 2 of the box rows
-        slab_rows_forward<NA, NB>(S, nk1, twB, lane, warp);
+        {   // forward FFT along axis 2 of the box rows
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) v[r] = valid ? row[P1 * (p + LB::N2 * r)] : make_float2(0.f, 0.f);
+                warp_line_fft<NB, false, P1>(v, p, valid, twB, row);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
         __syncthreads();
         slab_bulk_store<NB, P1>(slab, S, nk1, nk2, b2);   // ends with the barrier before S is reused
     }
