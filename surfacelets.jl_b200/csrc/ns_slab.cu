@@ -397,59 +397,6 @@ __device__ __forceinline__ void slab_bulk_store(float2* dst, const float2* S, in
     __syncthreads();
 }
 
-// Inverse FFT along axis 2 of the slab's box rows k1 < nk1 (columns outside
-// the box read as zero), in place.  When the box spans every k1 (nk1 =
-// NA/2 + 1), rows 0 and NA/2 hold Hermitian sequences along k2 (the slab of
-// a Hermitian spectrum), whose inverse transforms are real: they share one
-// complex line, row_0 + i row_NA/2, and its real and imaginary parts go back
-// to the two rows (imaginary parts 0, as the C2R along axis 1 reads them),
-// so the rows fit the CTA's lines in one round fewer.
-template <int NA, int NB>
-__device__ __forceinline__ void slab_rows_inverse(float2* S, int nk1, int b2, int k2hi, const float2* twB, int lane,
-                                                  int warp) {
-    using LB = SlabLine<NB>;
-    constexpr int P1 = slab_pitch_c(NA / 2 + 1);
-    const bool pack = nk1 == NA / 2 + 1;
-    const int nrows = pack ? nk1 - 1 : nk1;   // with pack, line 0 carries rows 0 and NA/2
-    const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
-    for (int base = 0; base < nrows; base += LB::LPR) {
-        if (base + warp * LB::LPW >= nrows) continue;   // warp-uniform
-        const int k1 = base + warp * LB::LPW + s;
-        const bool valid = k1 < nrows;
-        const bool two = pack && k1 == 0;
-        float2* row = S + (valid ? k1 : 0);
-        const float2* row2 = S + NA / 2;
-        float2 v[LB::N1];
-#pragma unroll
-        for (int r = 0; r < LB::N1; ++r) {
-            const int k2 = p + LB::N2 * r;
-            const bool in = valid && (k2 <= b2 || k2 >= k2hi);
-            float2 a = in ? row[P1 * k2] : make_float2(0.f, 0.f);
-            if (two) {
-                const float2 b = in ? row2[P1 * k2] : make_float2(0.f, 0.f);
-                a = make_float2(a.x - b.y, a.y + b.x);
-            }
-            v[r] = a;
-        }
-        warp_line_fft<NB, true, P1>(v, p, valid, twB, row);
-        if (valid) {
-#pragma unroll
-            for (int j = 0; j < LB::M; ++j)
-#pragma unroll
-                for (int k = 0; k < LB::N2; ++k) {
-                    const int o = P1 * ((p + LB::N2 * j) + LB::N1 * k);
-                    const float2 w = v[j * LB::N2 + k];
-                    if (two) {
-                        row[o] = make_float2(w.x, 0.f);
-                        S[NA / 2 + o] = make_float2(w.y, 0.f);
-                    } else {
-                        row[o] = w;
-                    }
-                }
-        }
-    }
-}
-
 // Analysis slab pass (inverse): spectra -> real volumes (element stride ES).
 // The exchange slots of a column pair are the pair's two columns read as one
 // run of 2 P1 >= NA values.
@@ -482,7 +429,29 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
         // 1. the box of the slab into shared memory
         slab_bulk_load<NB, P1>(S, src, nk1, nk2, b2, bar, phase, a.status);
         // 2. inverse FFT along axis 2 of the rows k1 < nk1; columns outside the box are zero
-        slab_rows_inverse<NA, NB>(S, nk1, b2, k2hi, twB, lane, warp);
+        {
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) {
+                    const int k2 = p + LB::N2 * r;
+                    const bool in = valid && (k2 <= b2 || k2 >= k2hi);
+                    v[r] = in ? row[P1 * k2] : make_float2(0.f, 0.f);
+                }
+                warp_line_fft<NB, true, P1>(v, p, valid, twB, row);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
         __syncthreads();
         // 3. C2R along axis 1, columns 2l and 2l+1 as one complex line; rows k1 >= nk1 are zero
         {
@@ -669,8 +638,29 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_shrink_kernel(Slab
         float2* slab = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         const float tau = a.tau[a.items[a.item0 + z].s - 1];
         slab_bulk_load<NB, P1>(S, slab, nk1, nk2, b2, bar, phase, a.status);
-        // inverse FFT along axis 2 of the box rows
-        slab_rows_inverse<NA, NB>(S, nk1, b2, k2hi, twB, lane, warp);
+        {   // inverse FFT along axis 2 of the box rows
+            const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
+            for (int base = 0; base < nk1; base += LB::LPR) {
+                if (base + warp * LB::LPW >= nk1) continue;   // warp-uniform
+                const int k1 = base + warp * LB::LPW + s;
+                const bool valid = k1 < nk1;
+                float2* row = S + (valid ? k1 : 0);
+                float2 v[LB::N1];
+#pragma unroll
+                for (int r = 0; r < LB::N1; ++r) {
+                    const int k2 = p + LB::N2 * r;
+                    const bool in = valid && (k2 <= b2 || k2 >= k2hi);
+                    v[r] = in ? row[P1 * k2] : make_float2(0.f, 0.f);
+                }
+                warp_line_fft<NB, true, P1>(v, p, valid, twB, row);
+                if (valid) {
+#pragma unroll
+                    for (int j = 0; j < LB::M; ++j)
+#pragma unroll
+                        for (int k = 0; k < LB::N2; ++k) row[P1 * ((p + LB::N2 * j) + LB::N1 * k)] = v[j * LB::N2 + k];
+                }
+            }
+        }
         __syncthreads();
         {   // per column pair: C2R, threshold, R2C
             const int p = lane & (LA::N2 - 1), s = pair_subline<NA>(lane / LA::N2);
