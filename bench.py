@@ -269,7 +269,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip plain/secondary/cpu legs")
     ap.add_argument("--group", type=int, default=0, help="subbands in flight per launch (0: the plan's default)")
-    ap.add_argument("--workspaces", type=int, default=4, help="graph mode: workspaces (concurrent branches, <= 16)")
+    ap.add_argument("--workspaces", type=int, default=4, help="graph mode: workspaces (concurrent branches, <= 8)")
     ap.add_argument("--dims", type=int, nargs=3, default=list(DIMS),
                     help="volume size (a smaller or larger case for profiling; the extra lines need the default)")
     ap.add_argument("--levels", type=int, nargs="+", default=NS_KW["direction_levels"],

@@ -356,7 +356,7 @@ int sfl_ns_synthesize_bf16(sfl_plan* plan, const void* c, const float* scales, v
 /* ── Batches ─────────────────────────────────────────────────────────────
  * Many transforms as one CUDA graph: batch_create runs each entry (plan,
  * operator, input, output) once eagerly, then captures the sequence
- * (distinct plans on up to 16 concurrent branches, each plan dealt out,
+ * (distinct plans on up to eight concurrent branches, each plan dealt out,
  * largest work first, to the branch with the least work so far; the entries
  * of one plan keep their order, so an entry may consume an earlier one's
  * output) and

@@ -3,7 +3,7 @@
 The reference runs a batch of volumes as a loop of plain analyze!/synthesize!
 calls.  Here `Batch(workspaces, inputs, outputs, ops)` runs each entry once,
 captures the whole sequence into a CUDA graph (distinct workspaces on up to
-16 concurrent branches, dealt out largest first to the least-loaded branch;
+eight concurrent branches, dealt out largest first to the least-loaded branch;
 the entries of one workspace keep their order, so one entry may consume
 another's output) and `run()` replays it: one launch for the batch.  The tensors stay bound to the graph; refill the inputs in
 place between runs.

@@ -1161,7 +1161,7 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, cons
         // distinct plans run on up to kBranches concurrent branches; one plan always on the same branch, the
         // plans dealt out largest first to the branch with the least work so far (longest-processing-time
         // order), the work of an entry estimated as voxels x (1 + coefficients per voxel)
-        constexpr int kBranches = 16;
+        constexpr int kBranches = 8;
         std::vector<const sfl_plan*> distinct;
         std::vector<double> work;
         std::vector<int> plan_of(n);

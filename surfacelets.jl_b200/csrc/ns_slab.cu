@@ -182,18 +182,32 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
         const float g = m0.low ? m0.lowc * m0.lowv[i] : m0.m[i * si];
         xg[r] = valid ? c_scale(xp[(long long)i * s3], g) : make_float2(0.f, 0.f);
     }
+    // per subband of the CTA: whether its plane a is constant along the line (applied after the FFT) and
+    // that plane's value here, looked up once ahead of the FFTs
+    const bool wedge_masks = !(synth && !tb.tight);
+    float a0s[IPC];
+    bool afters[IPC];
+#pragma unroll
+    for (int zz = 0; zz < IPC; ++zz) {
+        a0s[zz] = 1.f;
+        afters[zz] = false;
+        if (k0 + zz < nz) {
+            const NSItem* it = items + item0 + zof(k0 + zz);
+            afters[zz] = wedge_masks && it->kind == 0 && it->wa_hi != 2;
+            if (afters[zz]) a0s[zz] = ns_wedge_a_line(tb, it, k1, k2);
+        }
+    }
     float2 u[E];
 #pragma unroll 1
     for (int zz = 0; zz < IPC; ++zz) {
         const int k = k0 + zz;
         if (k >= nz) break;   // uniform across the CTA
         const int z = zof(k);
-        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
-        const bool wedges = !(mk.low || mk.plain);
-        // plane a constant along the line: applied after the FFT
-        const bool after = wedges && mk.was == 0;
+        const bool after = afters[zz];
         const bool reuse = after && nbq > 0 && zz > 0 && (k - 1) / rows == k / rows;   // same q: uniform
         if (!reuse) {
+            const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
+            const bool wedges = !(mk.low || mk.plain);
             float2 v[N1];
             if (!wedges) {
 #pragma unroll
@@ -215,7 +229,7 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
             reg_line_fft_v<N, true>(v, p, xl, tw, u);
         }
         if (valid) {
-            const float a0 = after ? mk.wa[0] : 1.f;
+            const float a0 = a0s[zz];
             float2* y = Y + z * ystride + k1 + P1 * k2;
 #pragma unroll
             for (int j = 0; j < Ge::M; ++j)
@@ -290,22 +304,62 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
     const int rows = nbq > 0 ? G / nbq : 1;
     const int nterms = nbq > 0 ? nbq : G;
     const float2* yl = Y + k1 + P1 * k2;
+    // whether an item's plane a is constant along the line (directional item, tight or analysis masks), and
+    // that plane's value at the line, for the first kPre items: looked up once, ahead of the loads they scale
+    constexpr int kPre = 8;
+    const bool wedge_masks = !(synth && !tb.tight);
+    float az_pre[kPre];
+#pragma unroll
+    for (int z = 0; z < kPre; ++z) {
+        az_pre[z] = 1.f;
+        if (z < G) {
+            const NSItem* it = items + item0 + z;
+            if (wedge_masks && it->kind == 0 && it->wa_hi != 2) az_pre[z] = ns_wedge_a_line(tb, it, k1, k2);
+        }
+    }
     for (int t = 0; t < nterms; ++t) {
-        // plane a constant along the line (directional item, tight or analysis masks): applied before the FFT
         const NSItem* it0 = items + item0 + t;
-        const bool before = it0->kind == 0 && !(synth && !tb.tight) && it0->wa_hi != 2;
-        // the term: sum_p wa_p Y_pq (one item with weight 1 when plane a varies along the line; x 1 is exact)
+        const bool before = wedge_masks && it0->kind == 0 && it0->wa_hi != 2;   // plane a applied before the FFT
+        // the term: sum_p wa_p Y_pq (one item with weight 1 when plane a varies along the line; x 1 is exact).
+        // The loads of the next item are in flight while the current one is added.
         const int nt = before ? rows : 1;
-        float2 v[N1];
+        float2 v[N1], yb[N1];
+        {
+            const float2* yz = yl + t * ystride;
+#pragma unroll
+            for (int r = 0; r < N1; ++r) yb[r] = valid ? yz[(long long)(p + N2 * r) * s3] : make_float2(0.f, 0.f);
+        }
 #pragma unroll 1
         for (int pp = 0; pp < nt; ++pp) {
             const int z = nbq > 0 ? pp * nbq + t : t;
-            const float az = before ? ns_wedge_a_line(tb, items + item0 + z, k1, k2) : 1.f;
-            const float2* yz = yl + z * ystride;
+            const float az = !before ? 1.f
+                                     : (z < kPre ? az_pre[z] : ns_wedge_a_line(tb, items + item0 + z, k1, k2));
+            if constexpr (N1 <= 16) {
+                // a second buffer for the next item's loads (long lines would spill it)
+                float2 cur[N1];
 #pragma unroll
-            for (int r = 0; r < N1; ++r) {
-                const float2 y = valid ? yz[(long long)(p + N2 * r) * s3] : make_float2(0.f, 0.f);
-                v[r] = pp == 0 ? c_scale(y, az) : make_float2(fmaf(y.x, az, v[r].x), fmaf(y.y, az, v[r].y));
+                for (int r = 0; r < N1; ++r) cur[r] = yb[r];
+                if (pp + 1 < nt) {
+                    const float2* yz = yl + (z + nbq) * ystride;
+#pragma unroll
+                    for (int r = 0; r < N1; ++r)
+                        yb[r] = valid ? yz[(long long)(p + N2 * r) * s3] : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int r = 0; r < N1; ++r)
+                    v[r] = pp == 0 ? c_scale(cur[r], az)
+                                   : make_float2(fmaf(cur[r].x, az, v[r].x), fmaf(cur[r].y, az, v[r].y));
+            } else {
+                if (pp > 0) {
+                    const float2* yz = yl + z * ystride;
+#pragma unroll
+                    for (int r = 0; r < N1; ++r)
+                        yb[r] = valid ? yz[(long long)(p + N2 * r) * s3] : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int r = 0; r < N1; ++r)
+                    v[r] = pp == 0 ? c_scale(yb[r], az)
+                                   : make_float2(fmaf(yb[r].x, az, v[r].x), fmaf(yb[r].y, az, v[r].y));
             }
         }
         float2 u[E];
