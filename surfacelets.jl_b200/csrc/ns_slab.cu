@@ -454,7 +454,9 @@ __device__ __forceinline__ void slab_bulk_store(float2* dst, const float2* S, in
 // Analysis slab pass (inverse): spectra -> real volumes (element stride ES).
 // The exchange slots of a column pair are the pair's two columns read as one
 // run of 2 P1 >= NA values.
-template <int NA, int NB, int ES, int MINB>
+// FULL: the box spans every row and column (nk1 = NA/2 + 1, nk2 = NB; the
+// finest scale), known at compile time so that the box predicates fold away.
+template <int NA, int NB, int ES, int MINB, bool FULL>
 __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArgs a) {
     using LA = SlabLine<NA>;
     using LB = SlabLine<NB>;
@@ -468,7 +470,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
     load_slab_twiddles<NA>(twA, a.twa);
     load_slab_twiddles<NB>(twB, a.twb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
+    const int nk1 = FULL ? NA / 2 + 1 : a.nk1, nk2 = FULL ? NB : a.nk2, b2 = FULL ? NB : a.b2;
     const int k2hi = NB - (nk2 - b2 - 1);   // first negative-frequency column in the box
     uint64_t* bar = slab_bar<NA, NB>(sm);
     uint32_t phase = 0;
@@ -825,10 +827,10 @@ constexpr int slab_minb() {
 
 // One CTA a unit up to the resident capacity; CTAs stride over the rest.
 // KIND: 0 the forward slab pass, 1 the inverse, 2 the denoiser's shrink pass.
-template <int KIND, int NA, int NB, int ES>
+template <int KIND, int NA, int NB, int ES, bool FULL>
 void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     constexpr int MINB = (slab_minb<NA>() == 2 && slab_minb<NB>() == 2) ? 2 : 1;
-    auto kern = KIND == 1 ? ns_slab_inv_kernel<NA, NB, ES, MINB>
+    auto kern = KIND == 1 ? ns_slab_inv_kernel<NA, NB, ES, MINB, FULL>
                           : (KIND == 0 ? ns_slab_fwd_kernel<NA, NB, ES, MINB> : ns_slab_shrink_kernel<NA, NB, MINB>);
     static size_t configured = 0;
     static int resident = 0;
@@ -850,10 +852,18 @@ void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, co
 template <int KIND, int NA, int NB>
 void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     if (a.P1 != slab_pitch_c(NA / 2 + 1)) throw ArgError("slab pitch mismatch");
-    if (a.es == 1)
-        launch_slab_es<KIND, NA, NB, 1>(a, sms, smem, st, tag);
-    else
-        launch_slab_es<KIND, NA, NB, 2>(a, sms, smem, st, tag);
+    const bool full = KIND == 1 && a.nk1 == NA / 2 + 1 && a.nk2 == NB;
+    if (a.es == 1) {
+        if (full)
+            launch_slab_es<KIND, NA, NB, 1, true>(a, sms, smem, st, tag);
+        else
+            launch_slab_es<KIND, NA, NB, 1, false>(a, sms, smem, st, tag);
+    } else {
+        if (full)
+            launch_slab_es<KIND, NA, NB, 2, true>(a, sms, smem, st, tag);
+        else
+            launch_slab_es<KIND, NA, NB, 2, false>(a, sms, smem, st, tag);
+    }
 }
 
 template <int KIND, int NA>
