@@ -862,6 +862,34 @@ struct RStoreCJobs {
     }
 };
 
+// Up to three line passes of one loader / store type as the jobs of one
+// register-pass launch (grid.y = job): each job keeps its own geometry, and
+// lines past a job's own count are invalid for it.
+template <class L>
+struct LoadJobs {
+    L j[3];
+    struct Ctx {
+        typename L::Ctx c;
+        int z;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const { return Ctx{j[z].line(0, l, valid), z}; }
+    __device__ __forceinline__ float2 get(const Ctx& c, int i) const { return j[c.z].get(c.c, i); }
+};
+template <class S>
+struct StoreJobs {
+    static constexpr bool kStaged = S::kStaged;
+    S j[3];
+    struct Ctx {
+        typename S::Ctx c;
+        int z;
+    };
+    __device__ __forceinline__ Ctx line(int z, int l, bool valid) const { return Ctx{j[z].line(0, l, valid), z}; }
+    __device__ __forceinline__ void put(const Ctx& c, int k, float2 v) const { j[c.z].put(c.c, k, v); }
+    __device__ __forceinline__ void staged(const Ctx& c, const float2* xl, int p, int n2) const {
+        j[c.z].staged(c.c, xl, p, n2);
+    }
+};
+
 // The block FFTs of every hourglass of level L along both transverse axes,
 // grouped into one launch per (block length, line layout); lengths without a
 // register pass run one segmented pass per spectrum and axis.
@@ -1104,17 +1132,30 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
     }
     // the block FFTs of the other hourglasses, grouped by length and layout
     block_fft_level(D, L, true, fuse, st);
+    // the C2R along K into the subbands: the hourglasses of one length and line layout in one launch
+    bool done[3] = {false, false, false};
     for (int K = 0; K < 3; ++K) {
-        float2* S = D.S[K].as<float2>();
-        Lines gk = k_lines(L, K);
+        if (done[K]) continue;
+        LoadJobs<RLoadHPair> lj{};
+        StoreJobs<RStoreRPairBlocks> sj{};
+        int nj = 0, pairs = 0;
+        for (int K2 = K; K2 < 3; ++K2) {
+            if (done[K2] || L.n[K2] != L.n[K] || (K2 != 0) != (K != 0)) continue;
+            Lines gk = k_lines(L, K2);
+            lj.j[nj] = RLoadHPair{D.S[K2].as<float2>(), ZMap{}, gk, L.n[K2]};
+            sj.j[nj] = RStoreRPairBlocks{c, block_map(L, K2), gk.nlines, es};
+            pairs = std::max(pairs, (gk.nlines + 1) / 2);
+            done[K2] = true;
+            ++nj;
+        }
         FFTLen* f = get_fft(D.ffts, L.n[K]);
-        BlockMap bm = block_map(L, K);
-        int pairs = (gk.nlines + 1) / 2;
-        if (!launch_reg<true>(L.n[K], RLoadHPair{S, ZMap{}, gk, L.n[K]}, RStoreRPairBlocks{c, bm, gk.nlines, es},
-                              f->sh.tw, pairs, 1, K != 0, st, "dec_c2r_blocks")) {
-            LoadHPair ld{S, ZMap{}, gk};
-            StoreRPairBlocks sto{c, bm, gk.nlines, es};
-            launch_pass(ld, sto, f->sh, pairs, 1, true, st, "dec_c2r_blocks");
+        if (!launch_reg<true>(L.n[K], lj, sj, f->sh.tw, pairs, nj, K != 0, st, "dec_c2r_blocks")) {
+            for (int t = 0; t < nj; ++t) {
+                const RLoadHPair& l1 = lj.j[t];
+                LoadHPair ld{l1.src, ZMap{}, l1.g};
+                StoreRPairBlocks sto{c, sj.j[t].bm, l1.g.nlines, es};
+                launch_pass(ld, sto, f->sh, (l1.g.nlines + 1) / 2, 1, true, st, "dec_c2r_blocks");
+            }
         }
     }
 }
@@ -1122,18 +1163,30 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
 void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
     HermArgs ha;
+    // the R2C along K out of the subbands: the hourglasses of one length and line layout in one launch
+    bool done[3] = {false, false, false};
     for (int K = 0; K < 3; ++K) {
-        const int* hd = L.hd[K];
-        float2* S = D.S[K].as<float2>();
-        Lines gk = k_lines(L, K);
+        if (done[K]) continue;
+        LoadJobs<RLoadRPairBlocks> lj{};
+        StoreJobs<RStoreHalfPair> sj{};
+        int nj = 0, pairs = 0;
+        for (int K2 = K; K2 < 3; ++K2) {
+            if (done[K2] || L.n[K2] != L.n[K] || (K2 != 0) != (K != 0)) continue;
+            Lines gk = k_lines(L, K2);
+            lj.j[nj] = RLoadRPairBlocks{c, block_map(L, K2), gk.nlines, es};
+            sj.j[nj] = RStoreHalfPair{D.S[K2].as<float2>(), ZMap{}, gk, L.n[K2]};
+            pairs = std::max(pairs, (gk.nlines + 1) / 2);
+            done[K2] = true;
+            ++nj;
+        }
         FFTLen* f = get_fft(D.ffts, L.n[K]);
-        BlockMap bm = block_map(L, K);
-        int pairs = (gk.nlines + 1) / 2;
-        if (!launch_reg<false>(L.n[K], RLoadRPairBlocks{c, bm, gk.nlines, es}, RStoreHalfPair{S, ZMap{}, gk, L.n[K]},
-                               f->sh.tw, pairs, 1, K != 0, st, "dec_r2c_blocks")) {
-            LoadRPairBlocks ld{c, bm, gk.nlines, es};
-            StoreHalfPair sto{S, ZMap{}, gk};
-            launch_pass(ld, sto, f->sh, pairs, 1, false, st, "dec_r2c_blocks");
+        if (!launch_reg<false>(L.n[K], lj, sj, f->sh.tw, pairs, nj, K != 0, st, "dec_r2c_blocks")) {
+            for (int t = 0; t < nj; ++t) {
+                const RStoreHalfPair& s1 = sj.j[t];
+                LoadRPairBlocks ld{c, lj.j[t].bm, s1.g.nlines, es};
+                StoreHalfPair sto{s1.dst, ZMap{}, s1.g};
+                launch_pass(ld, sto, f->sh, (s1.g.nlines + 1) / 2, 1, false, st, "dec_r2c_blocks");
+            }
         }
     }
     // the block FFTs of the hourglasses whose plane pass does not run them, grouped by length and layout
