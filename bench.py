@@ -166,6 +166,34 @@ def kernel_bytes(tag, P, launches_per_step, nz_total):
     return per_item * nz_total + extra * launches_per_step
 
 
+_SGEMM = []
+
+
+def sgemm_tflops():
+    """Measured FP32 peak: cuBLAS SGEMM of 8192^3 with TF32 off, best of five."""
+    if not _SGEMM:
+        import torch
+        prev = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = False
+        n = 8192
+        a = torch.randn(n, n, device="cuda")
+        b = torch.randn(n, n, device="cuda")
+        torch.matmul(a, b)
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        torch.backends.cuda.matmul.allow_tf32 = prev
+        del a, b
+        torch.cuda.empty_cache()
+        _SGEMM.append(2.0 * n ** 3 / (best / 1e3) / 1e12)
+    return _SGEMM[0]
+
+
 def host64(t):
     """A column-major device volume as a float64 NumPy array (Julia axis order)."""
     return np.asfortranarray(t.permute(*reversed(range(t.dim()))).cpu().numpy().transpose()).astype(np.float64)
@@ -445,17 +473,22 @@ def main():
         "kernel_algorithmic_gbs": {k: tag_bytes[k] / (v[0] / 1e3) / 1e9 for k, v in per_tag.items()
                                    if tag_bytes.get(k)},
     }
-    # The co-limit: FP32 FFT arithmetic on the CUDA cores.  Algorithmic FLOPs
-    # are the reference's unpruned cascade, 2.5 N log2 N a real 3-D FFT and
-    # (1 + S) FFTs an operator, three operators a volume; the peak is the
-    # nominal FMA rate (148 SMs x 128 lanes x 2 FLOP) at the sampled SM clock.
+    # The co-limit: FP32 arithmetic on the CUDA cores.  The FLOPs a voxel are
+    # measured (ncu thread-instruction counts FADD + FMUL + 2 FFMA over every
+    # launch of one step, profiles/fp32_flops.json) on the default workload;
+    # the peak is cuBLAS SGEMM (TF32 off) measured here, with the nominal FMA
+    # rate at the sampled SM clock beside it.
     mhz = clk["sm_mhz"] if clk else 1965.0
-    fft_flop = 3.0 * (1 + S) * 2.5 * N * np.log2(N) * B * world
-    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    fp32_ach = fft_flop / (ms / 1e3) / 1e12 / world
-    line["fp32_roofline"] = {"bound": "fp32", "algorithmic_flop_per_voxel": fft_flop / (N * B * world),
-                             "achieved": fp32_ach, "peak": fp32_peak, "unit": "TFLOP/s",
-                             "frac": fp32_ach / fp32_peak, "peak_kind": "nominal at the sampled SM clock"}
+    ffile = os.path.join(ROOT, "profiles", "fp32_flops.json")
+    if os.path.exists(ffile) and DIMS == (128, 128, 128) and S == 49:
+        flop_vox, flop_kind = json.load(open(ffile))["flop_per_voxel_step"], "measured (ncu, one step)"
+    else:
+        flop_vox, flop_kind = 3.0 * (1 + S) * 2.5 * np.log2(N), "estimate: 2.5 N log2 N a real 3-D FFT, unpruned"
+    fp32_ach = flop_vox * N * B / (ms / 1e3) / 1e12
+    line["fp32_roofline"] = {"bound": "fp32", "flop_per_voxel": flop_vox, "flop_kind": flop_kind,
+                             "achieved": fp32_ach, "peak": sgemm_tflops(), "unit": "TFLOP/s",
+                             "frac": fp32_ach / sgemm_tflops(), "peak_kind": "measured: cuBLAS SGEMM 8192^3, TF32 off",
+                             "nominal_fma_peak": 148 * 128 * 2 * mhz * 1e6 / 1e12}
     if clk:
         line["clocks"] = {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}
 
