@@ -159,32 +159,18 @@ __device__ __forceinline__ void mask_line_items(const float2 (&xg)[RegGeom<N>::N
     constexpr int N1 = Ge::N1, N2 = Ge::N2, E = Ge::M * Ge::N2;
     const int lnat = k1 + tb.h1 * k2;
     auto zof = [&](int k) { return nbq > 0 ? (k % rows) * nbq + k / rows : k; };
-    // per subband of the CTA: whether its plane a is constant along the line (applied after the FFT) and
-    // that plane's value here, looked up once ahead of the FFTs
-    const bool wedge_masks = !(synth && !tb.tight);
-    float a0s[IPC];
-    bool afters[IPC];
-#pragma unroll
-    for (int zz = 0; zz < IPC; ++zz) {
-        a0s[zz] = 1.f;
-        afters[zz] = false;
-        if (k0 + zz < nz) {
-            const NSItem* it = items + item0 + zof(k0 + zz);
-            afters[zz] = wedge_masks && it->kind == 0 && it->wa_hi != 2;
-            if (afters[zz]) a0s[zz] = ns_wedge_a_line(tb, it, k1, k2);
-        }
-    }
     float2 u[E];
 #pragma unroll 1
     for (int zz = 0; zz < IPC; ++zz) {
         const int k = k0 + zz;
         if (k >= nz) break;   // uniform across the CTA
         const int z = zof(k);
-        const bool after = afters[zz];
+        const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
+        const bool wedges = !(mk.low || mk.plain);
+        // plane a constant along the line: applied after the FFT
+        const bool after = wedges && mk.was == 0;
         const bool reuse = after && nbq > 0 && zz > 0 && (k - 1) / rows == k / rows;   // same q: uniform
         if (!reuse) {
-            const NSMaskLine mk = ns_mask_line(tb, items[item0 + z], lnat, synth != 0);
-            const bool wedges = !(mk.low || mk.plain);
             float2 v[N1];
             if (!wedges) {
 #pragma unroll
@@ -206,7 +192,7 @@ __device__ __forceinline__ void mask_line_items(const float2 (&xg)[RegGeom<N>::N
             reg_line_fft_v<N, true>(v, p, xl, tw, u);
         }
         if (valid) {
-            const float a0 = a0s[zz];
+            const float a0 = after ? mk.wa[0] : 1.f;
             float2* y = Y + z * ystride + k1 + P1 * k2;
 #pragma unroll
             for (int j = 0; j < Ge::M; ++j)
@@ -255,74 +241,6 @@ __global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_group_kernel
     }
     mask_line_items<N, IPC>(xg, valid, k1, k2, p, xl, tb, items, item0, nz, k0, nbq, rows, synth, Y, ystride, P1, s3,
                             tw);
-}
-
-// The same pass with persistent CTAs over the line blocks: each thread stages
-// its values of X and of the group factor for the CTA's next block in shared
-// memory with cp.async while the current block's FFTs run, and reads them
-// back after waiting on its own copies (no CTA barrier needed: every slot is
-// written and read by one thread).  Not for the lowpass (its factor is a
-// product of per-axis vectors).
-template <int N>
-constexpr size_t mask_pipe_smem() {
-    return RegGeom<N>::SMEM + (sizeof(float2) + sizeof(float)) * RegGeom<N>::N1 * 256;
-}
-
-template <int N, int IPC>
-__global__ void __launch_bounds__(256, mask_minb<N>()) ns_slab_mask_pipe_kernel(const float2* __restrict__ X, int P1, int s3,
-                                                                 BoxMap bx, NSMaskTables tb,
-                                                                 const NSItem* __restrict__ items, int item0, int nz,
-                                                                 int synth, float2* Y, long long ystride,
-                                                                 const float2* __restrict__ tw, int nlines,
-                                                                 long long xchs, long long ychs, int nbq) {
-    using Ge = RegGeom<N>;
-    constexpr int N1 = Ge::N1, N2 = Ge::N2, LP = Ge::LP;
-    extern __shared__ float2 xch[];
-    float2* xs = xch + LP * Ge::XLINE;                      // staged X: value r of thread t at [r * 256 + t]
-    float* gs = reinterpret_cast<float*>(xs + N1 * 256);    // staged group factor, the same layout
-    X += blockIdx.z * xchs;   // channel
-    Y += blockIdx.z * ychs;
-    const int tid = threadIdx.x;
-    const int lp = tid % LP, p = tid / LP;
-    float2* xl = xch + lp * Ge::XLINE;
-    const long long si = (long long)tb.h1 * tb.n2;
-    const int k0 = blockIdx.y * IPC;
-    const int rows = nbq > 0 ? nz / nbq : 0;
-    const int z0 = nbq > 0 ? (k0 % rows) * nbq + k0 / rows : k0;
-    // the group (or bandpass) table of the chunk, at the grid's origin
-    const float* gbase = ns_mask_line(tb, items[item0 + z0], 0, synth != 0).m;
-    const int nblocks = (nlines + LP - 1) / LP;
-    auto stage = [&](int blk) {
-        const int l = blk * LP + lp;
-        if (l < nlines) {
-            int k1, k2;
-            bx.k12(l, k1, k2);
-            const float2* xp = X + k1 + P1 * k2;
-            const float* gp = gbase + k1 + tb.h1 * k2;
-#pragma unroll
-            for (int r = 0; r < N1; ++r) {
-                const int i = p + N2 * r;
-                cp_async_8(xs + r * 256 + tid, xp + (long long)i * s3);
-                cp_async_4(gs + r * 256 + tid, gp + (long long)i * si);
-            }
-        }
-        cp_async_commit();
-    };
-    int blk = blockIdx.x;
-    if (blk < nblocks) stage(blk);
-    for (; blk < nblocks; blk += gridDim.x) {
-        const int l = blk * LP + lp;
-        const bool valid = l < nlines;
-        int k1 = 0, k2 = 0;
-        if (valid) bx.k12(l, k1, k2);
-        cp_async_wait_all();   // this thread's values of the block are in shared memory
-        float2 xg[N1];
-#pragma unroll
-        for (int r = 0; r < N1; ++r) xg[r] = valid ? c_scale(xs[r * 256 + tid], gs[r * 256 + tid]) : make_float2(0.f, 0.f);
-        if (blk + gridDim.x < nblocks) stage(blk + gridDim.x);   // the next block's loads run under this one's FFTs
-        mask_line_items<N, IPC>(xg, valid, k1, k2, p, xl, tb, items, item0, nz, k0, nbq, rows, synth, Y, ystride, P1,
-                                s3, tw);
-    }
 }
 
 // Synthesis line pass: FFT_3 of every item of a mask group, times its mask,
@@ -1044,17 +962,6 @@ void launch_slab_accum(const NSPlan& P, const float2* Y, int nz, const BoxMap& b
     cuda_check(cudaGetLastError(), "ns_slab_accum_kernel launch");
 }
 
-// The pipelined analysis axis-3 pass (persistent CTAs, cp.async staging) for
-// lines of up to 16 values a thread; SFL_MASK_PIPE=0 in the environment keeps
-// the one-block-a-CTA pass.
-bool mask_pipe_enabled_env() {
-    static const bool on = [] {
-        const char* e = std::getenv("SFL_MASK_PIPE");
-        return !(e && std::atoi(e) == 0);
-    }();
-    return on;
-}
-
 template <int N, int IPC>
 void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
                            int nlines, int nch, long long xchs, long long ychs, int nbq, cudaStream_t st) {
@@ -1067,26 +974,6 @@ void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, 
         configured = true;
     }
     const int nblocks = (nlines + Ge::LP - 1) / Ge::LP, ny = (nz + IPC - 1) / IPC;
-    const bool lowpass = P.items_host[i0].kind == 1;
-    if (!lowpass && RegGeom<N>::N1 <= 16 && mask_pipe_enabled_env()) {
-        static bool pconfigured = false;
-        if (!pconfigured) {
-            cuda_check(cudaFuncSetAttribute(ns_slab_mask_pipe_kernel<N, IPC>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mask_pipe_smem<N>()),
-                       "cudaFuncSetAttribute");
-            pconfigured = true;
-        }
-        // persistent CTAs: about two an SM in all, each over a stride of line blocks
-        const int gx = std::max(1, std::min(nblocks, (2 * P.sms) / std::max(1, ny * nch)));
-        dim3 grid(gx, ny, nch);
-        int tok = prof_begin("ns_slab_mask_axis3", st);
-        ns_slab_mask_pipe_kernel<N, IPC><<<grid, Ge::THREADS, mask_pipe_smem<N>(), st>>>(
-            X, P.P1, P.P1 * P.dims[1], bx, P.tb, P.items.as<NSItem>(), i0, nz, synth, Y, P.SP,
-            P.ffts.at(P.dims[2])->sh.tw, nlines, xchs, ychs, nbq);
-        prof_end(tok, st);
-        cuda_check(cudaGetLastError(), "ns_slab_mask_pipe_kernel launch");
-        return;
-    }
     dim3 grid(nblocks, ny, nch);
     int tok = prof_begin("ns_slab_mask_axis3", st);
     ns_slab_mask_group_kernel<N, IPC><<<grid, Ge::THREADS, Ge::SMEM, st>>>(
