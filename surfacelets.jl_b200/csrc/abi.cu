@@ -626,7 +626,7 @@ int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream) {
                         }
                     }
                 if (pick.pipeline == SFL_PIPELINE_SLABS)
-                    for (int ipc : {1, 2}) {
+                    for (int ipc : {1, 2, 8}) {
                         const float ms = time_it(pick.pipeline, pick.group, ipc);
                         if (ms < best) {
                             best = ms;
@@ -740,8 +740,8 @@ int sfl_plan_tile(sfl_plan* plan, int32_t set, int32_t* ipc) {
         sfl::NSPlan& N = ns_of(plan, "the axis-3 tile");
         need(ipc, "ipc");
         if (set) {
-            if (*ipc != 0 && *ipc != 1 && *ipc != 2 && *ipc != 4)
-                throw sfl::ArgError("subbands a CTA must be 1, 2 or 4 (0: the default), got " + std::to_string(*ipc));
+            if (*ipc != 0 && *ipc != 1 && *ipc != 2 && *ipc != 4 && *ipc != 8)
+                throw sfl::ArgError("subbands a CTA must be 1, 2, 4 or 8 (0: the default), got " + std::to_string(*ipc));
             N.ipc = *ipc;
         } else {
             *ipc = N.ipc;

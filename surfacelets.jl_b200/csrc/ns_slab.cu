@@ -986,23 +986,24 @@ void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, 
 // Subbands a CTA of the analysis line pass takes: the line's X and group
 // factor are loaded once for all of them.
 // Subbands a CTA of the analysis axis-3 pass: the plan's choice (the
-// autotuner's tile), else up to 4, or at most SFL_MASK_IPC (1, 2 or 4) from
-// the environment, read once.
+// autotuner's tile), else up to 4, or at most SFL_MASK_IPC (1, 2, 4 or 8)
+// from the environment, read once.
 int mask_ipc(const NSPlan& P, int nz) {
     static const int env_cap = [] {
         const char* e = std::getenv("SFL_MASK_IPC");
         const int v = e ? std::atoi(e) : 4;
-        return v >= 4 ? 4 : (v >= 2 ? 2 : 1);
+        return v >= 8 ? 8 : (v >= 4 ? 4 : (v >= 2 ? 2 : 1));
     }();
     const int cap = P.ipc > 0 ? P.ipc : env_cap;
     const int m = std::min(nz, cap);
-    return m >= 4 ? 4 : (m >= 2 ? 2 : 1);
+    return m >= 8 ? 8 : (m >= 4 ? 4 : (m >= 2 ? 2 : 1));
 }
 
 template <int N>
 void launch_mask_group(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
                        int nlines, int nch, long long xchs, long long ychs, int nbq, cudaStream_t st) {
     switch (mask_ipc(P, nz)) {
+        case 8: launch_mask_group_ipc<N, 8>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
         case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
         case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
         default: launch_mask_group_ipc<N, 1>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;

@@ -434,7 +434,7 @@ class Workspace:
 
     def tile(self, ipc=None):
         """Subbands a CTA of the slab pipeline's axis-3 analysis pass takes
-        (1, 2 or 4; 0 = the default): read, or set when ipc is given."""
+        (1, 2, 4 or 8; 0 = the default): read, or set when ipc is given."""
         v = C.c_int32(0 if ipc is None else int(ipc))
         check(lib.sfl_plan_tile(self._h, 0 if ipc is None else 1, C.byref(v)))
         return v.value

@@ -179,12 +179,12 @@ def test_axis3_tile_is_tunable_and_does_not_change_results(sfl):
     x = sfl.to_device(np.random.default_rng(12).standard_normal(dims).astype(np.float32))
     assert ws.tile() == 0
     ref = sfl.analyze(ws, x)
-    for ipc in (1, 2, 4):
+    for ipc in (1, 2, 4, 8):
         assert ws.tile(ipc) == ipc and ws.tile() == ipc
         assert torch.equal(sfl.analyze(ws, x), ref), ipc
-    with pytest.raises(sfl.ArgumentError, match="1, 2 or 4"):
+    with pytest.raises(sfl.ArgumentError, match="1, 2, 4 or 8"):
         ws.tile(3)
     ws.tile(0)
     ws.autotune(x)
-    assert ws.tile() in (0, 1, 2)
+    assert ws.tile() in (0, 1, 2, 8)
     assert torch.equal(sfl.analyze(ws, x), ref) or ws.tuning()[0] == "lines"
