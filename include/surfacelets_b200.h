@@ -207,7 +207,7 @@ int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline);
 int sfl_plan_tuning(const sfl_plan* plan, int32_t* pipeline, int32_t* group);
 
 /* The tile of the slab pipeline's axis-3 analysis pass: subbands a CTA takes
- * (1, 2, 4 or 8; 0 = the default, 4 or the SFL_MASK_IPC environment variable).
+ * (1, 2, 4 or 8; 0 = the default, 8 or the SFL_MASK_IPC environment variable).
  * set != 0 writes *ipc, else reads it.  The autotuner picks it after the
  * pipeline and group.  NS plans only.  No counterpart in the reference. */
 int sfl_plan_tile(sfl_plan* plan, int32_t set, int32_t* ipc);
@@ -215,7 +215,7 @@ int sfl_plan_tile(sfl_plan* plan, int32_t set, int32_t* ipc);
 /* Times analysis of x (into c, overwritten) followed by synthesis (into a
  * scratch volume of its own) under every pipeline that fits the size and
  * groups of 2, 4 and 8 subbands, then, on the slab pipeline, the axis-3 tile
- * of 1, 2 or 8 subbands a CTA against the default 4 (sfl_plan_tile); keeps the
+ * of 1, 2 or 4 subbands a CTA against the default 8 (sfl_plan_tile); keeps the
  * fastest and records it for the process: NS and NDFB plans created later
  * with the same transform, size and element type start with it.
  * Synchronizes; reallocates the plan's scratch.  No-op for decimated plans.

@@ -626,7 +626,7 @@ int sfl_plan_autotune(sfl_plan* plan, const void* x, void* c, void* stream) {
                         }
                     }
                 if (pick.pipeline == SFL_PIPELINE_SLABS)
-                    for (int ipc : {1, 2, 8}) {
+                    for (int ipc : {1, 2, 4}) {
                         const float ms = time_it(pick.pipeline, pick.group, ipc);
                         if (ms < best) {
                             best = ms;
