@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
 
 // Synthesis / rfft slab pass (forward): real volumes (element stride ES) ->
 // spectra (the box rows).
-template <int NA, int NB, int ES, int MINB>
+template <int NA, int NB, int ES, int MINB, bool FULL>
 __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArgs a) {
     using LA = SlabLine<NA>;
     using LB = SlabLine<NB>;
@@ -574,7 +574,8 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_fwd_kernel(SlabArg
     load_slab_twiddles<NB>(twB, a.twb);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nk1 = a.nk1, nk2 = a.nk2, b2 = a.b2;
+    // FULL: the box spans every row and column (as in the inverse pass)
+    const int nk1 = FULL ? NA / 2 + 1 : a.nk1, nk2 = FULL ? NB : a.nk2, b2 = FULL ? NB : a.b2;
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
         const int per = a.nzc * a.n3;
         const int ch = u / per, ur = u - ch * per;
@@ -831,7 +832,7 @@ template <int KIND, int NA, int NB, int ES, bool FULL>
 void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     constexpr int MINB = (slab_minb<NA>() == 2 && slab_minb<NB>() == 2) ? 2 : 1;
     auto kern = KIND == 1 ? ns_slab_inv_kernel<NA, NB, ES, MINB, FULL>
-                          : (KIND == 0 ? ns_slab_fwd_kernel<NA, NB, ES, MINB> : ns_slab_shrink_kernel<NA, NB, MINB>);
+                          : (KIND == 0 ? ns_slab_fwd_kernel<NA, NB, ES, MINB, FULL> : ns_slab_shrink_kernel<NA, NB, MINB>);
     static size_t configured = 0;
     static int resident = 0;
     if (configured < smem) {
@@ -852,7 +853,7 @@ void launch_slab_es(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, co
 template <int KIND, int NA, int NB>
 void launch_slab_nn(const SlabArgs& a, int sms, size_t smem, cudaStream_t st, const char* tag) {
     if (a.P1 != slab_pitch_c(NA / 2 + 1)) throw ArgError("slab pitch mismatch");
-    const bool full = KIND == 1 && a.nk1 == NA / 2 + 1 && a.nk2 == NB;
+    const bool full = KIND != 2 && a.nk1 == NA / 2 + 1 && a.nk2 == NB;
     if (a.es == 1) {
         if (full)
             launch_slab_es<KIND, NA, NB, 1, true>(a, sms, smem, st, tag);
