@@ -42,6 +42,7 @@ struct DecLevelDev {
     long long first_off[3];           // element offset of hourglass K's first subband
     long long blk_elems[3];
     int nsub[3];
+    DevMem S[3];                      // this level's half-K spectra S_K
 };
 
 struct DecPlan {
@@ -52,7 +53,6 @@ struct DecPlan {
     long long ncoef = 0;
     std::vector<std::unique_ptr<DecLevelDev>> lv;
     std::vector<std::unique_ptr<DevMem>> spectra;   // J + 1 full complex grids
-    DevMem S[3];                                   // half-K spectra of level 0 size
     std::map<int, std::unique_ptr<FFTLen>> ffts;
 };
 
@@ -218,11 +218,13 @@ struct IrcPlaneStages {
     const float2* f1[kIrcPlaneMaxStages];
 };
 
-// The planes of up to three hourglasses in one launch: job t owns the CTAs
-// [first, first + hd[K]) (one per k_K plane); the hourglasses' S_K are
-// separate buffers.
+// The planes of the hourglasses of every pyramid level in one launch: job t
+// owns the CTAs [first, first + hd[K]) (one per k_K plane); every hourglass of
+// every level has its own S_K buffer.
 struct IrcPlaneJob {
     float2* S;
+    const float2* X;   // analysis: the level's full spectrum, n0 x n1 x ...
+    int n0, n1;
     int K, first;
     int hd[3];
     const float* V;   // analysis: the hourglass mask V_K and the subband scale s
@@ -234,9 +236,10 @@ struct IrcPlaneJob {
     const float2* tw1;
     const float2* tw2;
 };
+constexpr int kIrcPlaneMaxJobs = 12;   // hourglasses of up to four pyramid levels
 struct IrcPlaneJobs {
     int n;
-    IrcPlaneJob job[3];
+    IrcPlaneJob job[kIrcPlaneMaxJobs];
 };
 
 // Plane pitch: the first transverse length rounded to 2 mod 4, so that lines
@@ -313,12 +316,13 @@ __device__ void irc_plane_load_twiddles(float2* tw2s, const float2* tw, int bs) 
 }
 
 template <bool SYNTH>
-__global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(IrcPlaneJobs jobs, const float2* __restrict__ X,
-                                                                     int n0, int n1) {
+__global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __grid_constant__ IrcPlaneJobs jobs) {
     extern __shared__ float2 pl[];
     int t0 = 0;
     while (t0 + 1 < jobs.n && (int)blockIdx.x >= jobs.job[t0 + 1].first) ++t0;
     const IrcPlaneJob& jb = jobs.job[t0];
+    const float2* __restrict__ X = jb.X;
+    const int n0 = jb.n0, n1 = jb.n1;
     float2* S = jb.S;
     const int K = jb.K;
     const float* __restrict__ V = jb.V;
@@ -727,10 +731,11 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
         m->alloc(sizeof(float2) * (size_t)n[0] * n[1] * n[2]);
         D->spectra.push_back(std::move(m));
     }
-    for (int K = 0; K < 3; ++K) {
-        const int* h = D->lv[0]->hd[K];
-        D->S[K].alloc(sizeof(float2) * (size_t)h[0] * h[1] * h[2]);
-    }
+    for (auto& L : D->lv)
+        for (int K = 0; K < 3; ++K) {
+            const int* h = L->hd[K];
+            L->S[K].alloc(sizeof(float2) * (size_t)h[0] * h[1] * h[2]);
+        }
     plan.dec.reset(D.release());
 }
 
@@ -921,7 +926,7 @@ void block_fft_level(DecPlan& D, DecLevelDev& L, bool inv, const bool skip[3], c
             if (inGroup[K] || earlier_pending) continue;
             inGroup[K] = true;
             member[jobs.n] = b;
-            jobs.base[jobs.n] = D.S[K].as<float2>();
+            jobs.base[jobs.n] = L.S[K].as<float2>();
             jobs.g[jobs.n] = block_lines(L.hd[K], items[b].m, items[b].bl);
             nlines = std::max(nlines, jobs.g[jobs.n].nlines);
             ++jobs.n;
@@ -1059,55 +1064,83 @@ void irc_plane_configure(size_t smem) {
     }
 }
 
-// One launch of the plane pass over the hourglasses of level L whose plane
-// fits (analysis: with the mask on load from the level spectrum X; synthesis:
-// hourglasses without stages have nothing to do).
+// Whether the plane pass of level L runs hourglass K (its plane fits; the
+// synthesis has nothing to do without stages) and whether it runs K's block
+// FFTs too.
 template <bool SYNTH>
-void irc_plane_launch(DecPlan& D, DecLevelDev& L, const float2* X, const bool fuse[3], cudaStream_t st) {
+bool irc_plane_runs(const DecLevelDev& L, int K) {
+    return irc_plane_fits(L, K) && !(SYNTH && L.stages[K].empty());
+}
+template <bool SYNTH>
+bool irc_plane_fuses(const DecLevelDev& L, int K) {
+    return irc_plane_runs<SYNTH>(L, K) && irc_plane_fuses_blocks(L, K);
+}
+
+// One launch of the plane pass over every level's hourglasses whose plane
+// fits (analysis: with the mask on load from the level spectrum; synthesis:
+// hourglasses without stages have nothing to do), the finest level's planes
+// first so that the coarser levels' smaller planes fill the last wave.
+template <bool SYNTH>
+void irc_plane_launch_levels(DecPlan& D, cudaStream_t st) {
     IrcPlaneJobs jobs{};
     size_t smem = 0;
     int blocks = 0;
-    for (int K = 0; K < 3; ++K) {
-        if (!irc_plane_fits(L, K) || (SYNTH && L.stages[K].empty())) continue;
-        IrcPlaneJob& jb = jobs.job[jobs.n++];
-        jb.S = D.S[K].as<float2>();
-        jb.K = K;
-        jb.first = blocks;
-        for (int d = 0; d < 3; ++d) jb.hd[d] = L.hd[K][d];
-        jb.V = L.V[K].as<float>();
-        int sb[3];
-        for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
-        jb.s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
-        jb.sg = irc_plane_stages(L, K, SYNTH);
-        if (fuse[K]) {
-            const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
-            jb.bs1 = L.bsize[K][m1];
-            jb.bs2 = L.bsize[K][m2];
-            jb.tw1 = get_fft(D.ffts, jb.bs1)->sh.tw;
-            jb.tw2 = get_fft(D.ffts, jb.bs2)->sh.tw;
+    auto flush = [&] {
+        if (jobs.n == 0) return;
+        irc_plane_configure<SYNTH>(smem);
+        int tok = prof_begin("dec_irc_plane", st);
+        irc_plane_kernel<SYNTH><<<blocks, kIrcPlaneThreads, smem, st>>>(jobs);
+        prof_end(tok, st);
+        cuda_check(cudaGetLastError(), "irc_plane_kernel");
+        jobs = IrcPlaneJobs{};
+        smem = 0;
+        blocks = 0;
+    };
+    for (int j = 0; j < D.J; ++j) {
+        DecLevelDev& L = *D.lv[j];
+        for (int K = 0; K < 3; ++K) {
+            if (!irc_plane_runs<SYNTH>(L, K)) continue;
+            if (jobs.n == kIrcPlaneMaxJobs) flush();
+            IrcPlaneJob& jb = jobs.job[jobs.n++];
+            jb.S = L.S[K].as<float2>();
+            jb.X = D.spectra[j]->as<float2>();
+            jb.n0 = L.n[0];
+            jb.n1 = L.n[1];
+            jb.K = K;
+            jb.first = blocks;
+            for (int d = 0; d < 3; ++d) jb.hd[d] = L.hd[K][d];
+            jb.V = L.V[K].as<float>();
+            int sb[3];
+            for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
+            jb.s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
+            jb.sg = irc_plane_stages(L, K, SYNTH);
+            if (irc_plane_fuses<SYNTH>(L, K)) {
+                const int m1 = K == 0 ? 1 : 0, m2 = K == 2 ? 1 : 2;
+                jb.bs1 = L.bsize[K][m1];
+                jb.bs2 = L.bsize[K][m2];
+                jb.tw1 = get_fft(D.ffts, jb.bs1)->sh.tw;
+                jb.tw2 = get_fft(D.ffts, jb.bs2)->sh.tw;
+            }
+            blocks += L.hd[K][K];
+            smem = std::max(smem, irc_plane_smem(L, K));
         }
-        blocks += L.hd[K][K];
-        smem = std::max(smem, irc_plane_smem(L, K));
     }
-    if (jobs.n == 0) return;
-    irc_plane_configure<SYNTH>(smem);
-    int tok = prof_begin("dec_irc_plane", st);
-    irc_plane_kernel<SYNTH><<<blocks, kIrcPlaneThreads, smem, st>>>(jobs, X, L.n[0], L.n[1]);
-    prof_end(tok, st);
-    cuda_check(cudaGetLastError(), "irc_plane_kernel");
+    flush();
 }
 
+// Level j of the analysis after the plane pass (irc_plane_launch_levels<false>,
+// which ran the mask, every stage and, where both lengths allow, the block
+// FFTs of each hourglass whose plane fits): the other hourglasses' mask and
+// stages, the block FFTs the plane pass did not run, and the C2R along K
+// into the subbands.
 void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
     const float2* X = D.spectra[j]->as<float2>();
-    // mask, every stage and (where both lengths allow) the block FFTs of each hourglass whose plane fits:
-    // one pass over the k_K planes of all three
     bool fuse[3];
-    for (int K = 0; K < 3; ++K) fuse[K] = irc_plane_fits(L, K) && irc_plane_fuses_blocks(L, K);
-    irc_plane_launch<false>(D, L, X, fuse, st);
+    for (int K = 0; K < 3; ++K) fuse[K] = irc_plane_fuses<false>(L, K);
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
-        float2* S = D.S[K].as<float2>();
+        float2* S = L.S[K].as<float2>();
         int sb[3];
         for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
         float s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
@@ -1142,7 +1175,7 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
         for (int K2 = K; K2 < 3; ++K2) {
             if (done[K2] || L.n[K2] != L.n[K] || (K2 != 0) != (K != 0)) continue;
             Lines gk = k_lines(L, K2);
-            lj.j[nj] = RLoadHPair{D.S[K2].as<float2>(), ZMap{}, gk, L.n[K2]};
+            lj.j[nj] = RLoadHPair{L.S[K2].as<float2>(), ZMap{}, gk, L.n[K2]};
             sj.j[nj] = RStoreRPairBlocks{c, block_map(L, K2), gk.nlines, es};
             pairs = std::max(pairs, (gk.nlines + 1) / 2);
             done[K2] = true;
@@ -1160,9 +1193,13 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
     }
 }
 
+// Level j of the synthesis up to the plane pass (irc_plane_launch_levels<true>,
+// which runs every stage, in reverse, and where both lengths allow the block
+// FFTs before them, of each hourglass whose plane fits): the R2C along K out
+// of the subbands, the block FFTs the plane pass does not run and the other
+// hourglasses' stages.
 void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
-    HermArgs ha;
     // the R2C along K out of the subbands: the hourglasses of one length and line layout in one launch
     bool done[3] = {false, false, false};
     for (int K = 0; K < 3; ++K) {
@@ -1174,7 +1211,7 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
             if (done[K2] || L.n[K2] != L.n[K] || (K2 != 0) != (K != 0)) continue;
             Lines gk = k_lines(L, K2);
             lj.j[nj] = RLoadRPairBlocks{c, block_map(L, K2), gk.nlines, es};
-            sj.j[nj] = RStoreHalfPair{D.S[K2].as<float2>(), ZMap{}, gk, L.n[K2]};
+            sj.j[nj] = RStoreHalfPair{L.S[K2].as<float2>(), ZMap{}, gk, L.n[K2]};
             pairs = std::max(pairs, (gk.nlines + 1) / 2);
             done[K2] = true;
             ++nj;
@@ -1191,12 +1228,11 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
     }
     // the block FFTs of the hourglasses whose plane pass does not run them, grouped by length and layout
     bool fuse[3];
-    for (int K = 0; K < 3; ++K)
-        fuse[K] = irc_plane_fits(L, K) && !L.stages[K].empty() && irc_plane_fuses_blocks(L, K);
+    for (int K = 0; K < 3; ++K) fuse[K] = irc_plane_fuses<true>(L, K);
     block_fft_level(D, L, false, fuse, st);
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
-        float2* S = D.S[K].as<float2>();
+        float2* S = L.S[K].as<float2>();
         long long tot = (long long)hd[0] * hd[1] * hd[2];
         if (!irc_plane_fits(L, K)) {
             for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
@@ -1211,11 +1247,18 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
                 cuda_check(cudaGetLastError(), "irc_stage_kernel");
             }
         }
-        ha.S[K] = S;
+    }
+}
+
+// Level j of the synthesis after the plane pass: the Hermitian sum of its
+// three hourglasses into the level spectrum.
+void scale_inverse_sum(DecPlan& D, int j, cudaStream_t st) {
+    DecLevelDev& L = *D.lv[j];
+    HermArgs ha;
+    for (int K = 0; K < 3; ++K) {
+        ha.S[K] = L.S[K].as<float2>();
         ha.V[K] = L.V[K].as<float>();
     }
-    // every stage, in reverse, of each hourglass whose plane fits: one pass over the k_K planes of all three
-    irc_plane_launch<true>(D, L, nullptr, fuse, st);
     long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
     {
         int tok = prof_begin("dec_herm_sum", st);
@@ -1237,7 +1280,7 @@ void scale_forward_adjoint(DecPlan& D, int j, const float* c, int es, cudaStream
     float sK[3];
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
-        float2* S = D.S[K].as<float2>();
+        float2* S = L.S[K].as<float2>();
         Lines gk = k_lines(L, K);
         FFTLen* f = get_fft(D.ffts, L.n[K]);
         BlockMap bm = block_map(L, K);
@@ -1282,7 +1325,7 @@ void scale_inverse_adjoint(DecPlan& D, int j, float* c, int es, cudaStream_t st)
     DecLevelDev& L = *D.lv[j];
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
-        float2* S = D.S[K].as<float2>();
+        float2* S = L.S[K].as<float2>();
         long long tot = (long long)hd[0] * hd[1] * hd[2];
         {
             int tok = prof_begin("dec_herm_gather", st);
@@ -1329,10 +1372,11 @@ void dec_analyze(DecPlan& D, const void* x, void* c, cudaStream_t st) {
         const float* xin = reinterpret_cast<const float*>(x) + ch;
         float* cout = reinterpret_cast<float*>(c) + ch;
         fft_real_full(D, xin, es, D.dims, D.spectra[0]->as<float2>(), st);
-        for (int j = 0; j < D.J; ++j) {
-            pyr_split(D, j, st);
-            scale_forward(D, j, cout, es, st);
-        }
+        // every split first (split j leaves level j's highpass in spectrum j), so
+        // that one plane pass covers the hourglasses of all levels
+        for (int j = 0; j < D.J; ++j) pyr_split(D, j, st);
+        irc_plane_launch_levels<false>(D, st);
+        for (int j = 0; j < D.J; ++j) scale_forward(D, j, cout, es, st);
         const int* nl = S.pyramid[D.J - 1].nlow;
         float scale = (float)(1.0 / ((double)nl[0] * nl[1] * nl[2]));
         ifft_full_real(D, D.spectra[D.J]->as<float2>(), nl, cout, es, scale, st);
@@ -1347,8 +1391,10 @@ void dec_synthesize(DecPlan& D, const void* c, void* x, cudaStream_t st) {
         float* xout = reinterpret_cast<float*>(x) + ch;
         const int* nl = S.pyramid[D.J - 1].nlow;
         fft_real_full(D, cin, es, nl, D.spectra[D.J]->as<float2>(), st);
+        for (int j = D.J - 1; j >= 0; --j) scale_inverse(D, j, cin, es, st);
+        irc_plane_launch_levels<true>(D, st);
         for (int j = D.J - 1; j >= 0; --j) {
-            scale_inverse(D, j, cin, es, st);
+            scale_inverse_sum(D, j, st);
             pyr_merge(D, j, st);
         }
         float scale = (float)(1.0 / ((double)D.dims[0] * D.dims[1] * D.dims[2]));
