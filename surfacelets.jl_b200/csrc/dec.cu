@@ -93,24 +93,45 @@ __device__ __forceinline__ long long lin3(int a, int b, int c, int d0, int d1) {
     return a + (long long)d0 * (b + (long long)d1 * c);
 }
 
+// Unsigned division by a divisor fixed for a loop: n / d = umulhi(n, m) with
+// m = ceil(2^32 / d), after Granlund and Montgomery, "Division by invariant
+// integers using multiplication" (1994).  Exact when d is a power of two or
+// n * d < 2^32 (n / d gains less than n (d - 2^32 mod d) / (d 2^32) < 1/d);
+// the plane pass divides point and pair indices below 2^17 by lengths below
+// 2^12.
+struct FastDiv {
+    unsigned d, m;
+    __host__ __device__ explicit FastDiv(unsigned dv) : d(dv), m(dv > 1 ? 0xFFFFFFFFu / dv + 1u : 0u) {}
+    __device__ __forceinline__ unsigned div(unsigned n) const { return d > 1 ? __umulhi(n, m) : n; }
+};
+
+// The grid kernels below take one point each: a 32 x 8 block over the first two
+// axes, blockIdx.z over the third (no index division).
+constexpr int kGridBX = 32, kGridBY = 8;
+inline dim3 grid3_blocks(int d0, int d1, int d2) {
+    return dim3((unsigned)((d0 + kGridBX - 1) / kGridBX), (unsigned)((d1 + kGridBY - 1) / kGridBY), (unsigned)d2);
+}
+inline dim3 grid3_threads() { return dim3(kGridBX, kGridBY); }
+__device__ __forceinline__ bool grid3_point(int d0, int d1, int& a, int& b, int& c) {
+    a = blockIdx.x * kGridBX + threadIdx.x;
+    b = blockIdx.y * kGridBY + threadIdx.y;
+    c = blockIdx.z;
+    return a < d0 && b < d1;
+}
+
 // src/pyramid/fourier_pyramid.jl:221-231 (file numbering): low = crop(L X)/D^1.5,
 // X[box] *= sqrt(1 - L^2).  `low` must be zeroed first.
 // lw[q] = L D^-1.5 and hw[q] = sqrt(1 - L^2) on the box, designed in float64.
 __global__ void pyr_split_kernel(float2* X, float2* low, int n0, int n1, int l0, int l1, const int* i0,
                                  const int* i1, const int* i2, const int* j0, const int* j1, const int* j2,
                                  const float* lw, const float* hw, int c0, int c1, int c2) {
-    long long total = (long long)c0 * c1 * c2;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
-        int a = q % c0;
-        long long r = q / c0;
-        int b = r % c1;
-        int c = r / c1;
-        long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
-        float2 v = X[xa];
-        low[lin3(j0[a], j1[b], j2[c], l0, l1)] = c_scale(v, lw[q]);
-        X[xa] = c_scale(v, hw[q]);
-    }
+    int a, b, c;
+    if (!grid3_point(c0, c1, a, b, c)) return;
+    const long long q = lin3(a, b, c, c0, c1);
+    long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
+    float2 v = X[xa];
+    low[lin3(j0[a], j1[b], j2[c], l0, l1)] = c_scale(v, lw[q]);
+    X[xa] = c_scale(v, hw[q]);
 }
 
 // src/pyramid/fourier_pyramid.jl:235-240: X[box] = sqrt(1-L^2) X[box] + L D^1.5 low.
@@ -118,32 +139,22 @@ __global__ void pyr_split_kernel(float2* X, float2* low, int n0, int n1, int l0,
 __global__ void pyr_merge_kernel(float2* X, const float2* low, int n0, int n1, int l0, int l1, const int* i0,
                                  const int* i1, const int* i2, const int* j0, const int* j1, const int* j2,
                                  const float* lw, const float* hw, int c0, int c1, int c2) {
-    long long total = (long long)c0 * c1 * c2;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
-        int a = q % c0;
-        long long r = q / c0;
-        int b = r % c1;
-        int c = r / c1;
-        long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
-        float2 h = c_scale(X[xa], hw[q]);
-        float2 w = c_scale(low[lin3(j0[a], j1[b], j2[c], l0, l1)], lw[q]);
-        X[xa] = c_add(h, w);
-    }
+    int a, b, c;
+    if (!grid3_point(c0, c1, a, b, c)) return;
+    const long long q = lin3(a, b, c, c0, c1);
+    long long xa = lin3(i0[a], i1[b], i2[c], n0, n1);
+    float2 h = c_scale(X[xa], hw[q]);
+    float2 w = c_scale(low[lin3(j0[a], j1[b], j2[c], l0, l1)], lw[q]);
+    X[xa] = c_add(h, w);
 }
 
 // S_K = X[half_K] * V_K * s: src/directional/surfacelet_scale.jl:205-206, 292
 __global__ void hg_mask_kernel(const float2* X, int n0, int n1, float2* S, int h0, int h1, int h2,
                                const float* V, float s) {
-    long long total = (long long)h0 * h1 * h2;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
-        int a = q % h0;
-        long long r = q / h0;
-        int b = r % h1;
-        int c = r / h1;
-        S[q] = c_scale(X[lin3(a, b, c, n0, n1)], V[q] * s);
-    }
+    int a, b, c;
+    if (!grid3_point(h0, h1, a, b, c)) return;
+    const long long q = lin3(a, b, c, h0, h1);
+    S[q] = c_scale(X[lin3(a, b, c, n0, n1)], V[q] * s);
 }
 
 // One IRC stage in place on S (half-K dims h): for every bin pair (A, B) of
@@ -159,15 +170,10 @@ __global__ void irc_stage_kernel(float2* S, int h0, int h1, int h2, int K, int m
     int hd[3] = {h0, h1, h2};
     int pd[3] = {h0, h1, h2};
     pd[m] = hd[m] / 2;
-    long long total = (long long)pd[0] * pd[1] * pd[2];
     const int nKh = hd[K];
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
+    {
         int c[3];
-        c[0] = q % pd[0];
-        long long r = q / pd[0];
-        c[1] = r % pd[1];
-        c[2] = r / pd[1];
+        if (!grid3_point(pd[0], pd[1], c[0], c[1], c[2])) return;
         int pq = c[m];
         int cA = (pq / b) * 2 * b + (pq % b);
         int cB = cA + b;
@@ -340,6 +346,7 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __gri
     const long long base = (long long)kK * sK;
     const long long xbase = (long long)kK * xK;
     const int tot = a1 * a2;
+    const FastDiv fa1((unsigned)a1);
     const int ap = irc_plane_pitch(a1);                  // the plane's row pitch in shared memory
     float2* cf = pl + (long long)ap * a2;                // a stage's two filter rows
     float2* tws = cf + 2 * (a1 > a2 ? a1 : a2);          // block-FFT twiddles: bs1 then bs2 entries
@@ -356,7 +363,7 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __gri
             const int q = q0 + u * blockDim.x;
             v[u] = make_float2(0.f, 0.f);
             if (q < tot) {
-                const int i1 = q % a1, i2 = q / a1;
+                const int i2 = (int)fa1.div((unsigned)q), i1 = q - i2 * a1;
                 const long long g = base + i1 * s1 + i2 * s2;
                 if (!SYNTH) {
                     v[u] = c_scale(X[xbase + i1 * xa + i2 * xb], V[g] * s);
@@ -368,7 +375,10 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __gri
 #pragma unroll
         for (int u = 0; u < kIrcPlaneBatch; ++u) {
             const int q = q0 + u * blockDim.x;
-            if (q < tot) pl[(q % a1) + ap * (q / a1)] = v[u];
+            if (q < tot) {
+                const int i2 = (int)fa1.div((unsigned)q);
+                pl[(q - i2 * a1) + ap * i2] = v[u];
+            }
         }
     }
     __syncthreads();
@@ -385,6 +395,7 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __gri
         const bool first = sg.m[u] == (K == 0 ? 1 : 0);   // along the plane's first axis m1
         const int half = (first ? a1 : a2) / 2;
         const int npairs = half * (first ? a2 : a1);
+        const FastDiv fo((unsigned)(first ? half : a1)), fb((unsigned)b);
         // the stage's filter row at k_K (over the stage's axis) into shared memory
         const int am = first ? a1 : a2;
         for (int i = threadIdx.x; i < am; i += blockDim.x) {
@@ -395,15 +406,10 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __gri
         for (int q = threadIdx.x; q < npairs; q += blockDim.x) {
             // consecutive threads on consecutive words of the plane: the pair index runs fastest along
             // the first axis, the other index along the second
-            int pq, o;
-            if (first) {
-                pq = q % half;
-                o = q / half;
-            } else {
-                o = q % a1;
-                pq = q / a1;
-            }
-            const int cA = (pq / b) * 2 * b + (pq % b), cB = cA + b;
+            const int qd = (int)fo.div((unsigned)q), qr = q - qd * (int)fo.d;
+            const int pq = first ? qr : qd, o = first ? qd : qr;
+            const int pb = (int)fb.div((unsigned)pq);
+            const int cA = pb * 2 * b + (pq - pb * b), cB = cA + b;
             const int qA = first ? cA + ap * o : o + ap * cA;
             const int qB = first ? cB + ap * o : o + ap * cB;
             const float2 A = pl[qA], Bv = pl[qB];
@@ -429,7 +435,7 @@ __global__ void __launch_bounds__(kIrcPlaneThreads) irc_plane_kernel(const __gri
         __syncthreads();
     }
     for (int q = threadIdx.x; q < tot; q += blockDim.x) {
-        const int i1 = q % a1, i2 = q / a1;
+        const int i2 = (int)fa1.div((unsigned)q), i1 = q - i2 * a1;
         S[base + i1 * s1 + i2 * s2] = pl[i1 + ap * i2];
     }
 }
@@ -441,15 +447,11 @@ struct HermArgs {
     const float* V[3];
 };
 __global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs ha, float third) {
-    long long total = (long long)n0 * n1 * n2;
     int n[3] = {n0, n1, n2};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
+    {
         int k[3];
-        k[0] = q % n0;
-        long long r = q / n0;
-        k[1] = r % n1;
-        k[2] = r / n1;
+        if (!grid3_point(n0, n1, k[0], k[1], k[2])) return;
+        const long long q = lin3(k[0], k[1], k[2], n0, n1);
         float2 v = make_float2(0.f, 0.f);
 #pragma unroll
         for (int K = 0; K < 3; ++K) {
@@ -459,7 +461,7 @@ __global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs
                 long long a = lin3(k[0], k[1], k[2], hd[0], hd[1]);
                 v = c_add(v, c_scale(ha.S[K][a], third * ha.V[K][a]));
             } else {
-                int m0 = (n0 - k[0]) % n0, m1 = (n1 - k[1]) % n1, m2 = (n2 - k[2]) % n2;
+                const int m0 = k[0] ? n0 - k[0] : 0, m1 = k[1] ? n1 - k[1] : 0, m2 = k[2] ? n2 - k[2] : 0;
                 long long a = lin3(m0, m1, m2, hd[0], hd[1]);
                 v = c_add(v, c_scale(c_conj(ha.S[K][a]), third * ha.V[K][a]));
             }
@@ -471,16 +473,12 @@ __global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs
 // Adjoint of the hourglass masks of the analysis: X = sum_K pad_K(V_K s_K S_K),
 // zero outside each half grid.
 __global__ void hg_adjoint_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs ha, float s0, float s1, float s2) {
-    long long total = (long long)n0 * n1 * n2;
     int n[3] = {n0, n1, n2};
     const float sK[3] = {s0, s1, s2};
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
+    {
         int k[3];
-        k[0] = q % n0;
-        long long r = q / n0;
-        k[1] = r % n1;
-        k[2] = r / n1;
+        if (!grid3_point(n0, n1, k[0], k[1], k[2])) return;
+        const long long q = lin3(k[0], k[1], k[2], n0, n1);
         float2 v = make_float2(0.f, 0.f);
 #pragma unroll
         for (int K = 0; K < 3; ++K) {
@@ -503,18 +501,14 @@ __global__ void herm_gather_kernel(const float2* X, int n0, int n1, int n2, floa
     int n[3] = {n0, n1, n2};
     int hd[3] = {n0, n1, n2};
     hd[K] = n[K] / 2 + 1;
-    long long total = (long long)hd[0] * hd[1] * hd[2];
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
+    {
         int a[3];
-        a[0] = q % hd[0];
-        long long r = q / hd[0];
-        a[1] = r % hd[1];
-        a[2] = r / hd[1];
+        if (!grid3_point(hd[0], hd[1], a[0], a[1], a[2])) return;
+        const long long q = lin3(a[0], a[1], a[2], hd[0], hd[1]);
         float2 v = X[lin3(a[0], a[1], a[2], n0, n1)];
-        const int mK = (n[K] - a[K]) % n[K];
+        const int mK = a[K] ? n[K] - a[K] : 0;
         if (mK >= hd[K]) {
-            int m0 = (n0 - a[0]) % n0, m1 = (n1 - a[1]) % n1, m2 = (n2 - a[2]) % n2;
+            const int m0 = a[0] ? n0 - a[0] : 0, m1 = a[1] ? n1 - a[1] : 0, m2 = a[2] ? n2 - a[2] : 0;
             v = c_add(v, c_conj(X[lin3(m0, m1, m2, n0, n1)]));
         }
         S[q] = c_scale(v, third * V[q]);
@@ -742,6 +736,14 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
 // ── drivers ──────────────────────────────────────────────────────────────────
 
 namespace {
+
+// The grid of irc_stage_kernel: one thread a bin pair, over S_K's dims with
+// axis m halved.
+dim3 irc_stage_grid(const int* hd, int m) {
+    int pd[3] = {hd[0], hd[1], hd[2]};
+    pd[m] /= 2;
+    return grid3_blocks(pd[0], pd[1], pd[2]);
+}
 
 unsigned grid_for(long long total) {
     long long g = (total + 255) / 256;
@@ -989,10 +991,9 @@ void pyr_split(DecPlan& D, int j, cudaStream_t st, bool adjoint = false) {
     float2* X = D.spectra[j]->as<float2>();
     float2* low = D.spectra[j + 1]->as<float2>();
     cuda_check(cudaMemsetAsync(low, 0, D.spectra[j + 1]->bytes, st), "memset");
-    long long tot = (long long)L.cnt[0] * L.cnt[1] * L.cnt[2];
     {
         int tok = prof_begin("dec_pyr_split", st);
-        pyr_split_kernel<<<grid_for(tot), 256, 0, st>>>(
+        pyr_split_kernel<<<grid3_blocks(L.cnt[0], L.cnt[1], L.cnt[2]), grid3_threads(), 0, st>>>(
             X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
             L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(),
             adjoint ? L.lw_merge.as<float>() : L.lw_split.as<float>(), L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
@@ -1007,10 +1008,9 @@ void pyr_merge(DecPlan& D, int j, cudaStream_t st, bool adjoint = false) {
     DecLevelDev& L = *D.lv[j];
     float2* X = D.spectra[j]->as<float2>();
     const float2* low = D.spectra[j + 1]->as<float2>();
-    long long tot = (long long)L.cnt[0] * L.cnt[1] * L.cnt[2];
     {
         int tok = prof_begin("dec_pyr_merge", st);
-        pyr_merge_kernel<<<grid_for(tot), 256, 0, st>>>(
+        pyr_merge_kernel<<<grid3_blocks(L.cnt[0], L.cnt[1], L.cnt[2]), grid3_threads(), 0, st>>>(
             X, low, L.n[0], L.n[1], L.nlow[0], L.nlow[1], L.idx[0].as<int>(), L.idx[1].as<int>(), L.idx[2].as<int>(),
             L.idx_low[0].as<int>(), L.idx_low[1].as<int>(), L.idx_low[2].as<int>(),
             adjoint ? L.lw_split.as<float>() : L.lw_merge.as<float>(), L.hw.as<float>(), L.cnt[0], L.cnt[1], L.cnt[2]);
@@ -1144,19 +1144,17 @@ void scale_forward(DecPlan& D, int j, float* c, int es, cudaStream_t st) {
         int sb[3];
         for (int d = 0; d < 3; ++d) sb[d] = d == K ? L.n[K] : L.bsize[K][d];
         float s = (float)(1.0 / ((double)sb[0] * sb[1] * sb[2]));
-        long long tot = (long long)hd[0] * hd[1] * hd[2];
         if (!irc_plane_fits(L, K)) {
             int tok = prof_begin("dec_hg_mask", st);
-            hg_mask_kernel<<<grid_for(tot), 256, 0, st>>>(X, L.n[0], L.n[1], S, hd[0], hd[1], hd[2], L.V[K].as<float>(), s);
+            hg_mask_kernel<<<grid3_blocks(hd[0], hd[1], hd[2]), grid3_threads(), 0, st>>>(
+                X, L.n[0], L.n[1], S, hd[0], hd[1], hd[2], L.V[K].as<float>(), s);
             prof_end(tok, st);
             cuda_check(cudaGetLastError(), "hg_mask_kernel");
             for (auto& sg : L.stages[K]) {
-                long long pairs = tot / 2;
                 {
                     int tok = prof_begin("dec_irc", st);
-                    irc_stage_kernel<<<grid_for(pairs), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
-                                                                      sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0,
-                                                                      0);
+                    irc_stage_kernel<<<irc_stage_grid(hd, sg.m), grid3_threads(), 0, st>>>(
+                        S, hd[0], hd[1], hd[2], K, sg.m, sg.b, sg.f[0].as<float2>(), sg.f[1].as<float2>(), 0, 0);
                     prof_end(tok, st);
                 }
                 cuda_check(cudaGetLastError(), "irc_stage_kernel");
@@ -1233,13 +1231,12 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
         float2* S = L.S[K].as<float2>();
-        long long tot = (long long)hd[0] * hd[1] * hd[2];
         if (!irc_plane_fits(L, K)) {
             for (int s = (int)L.stages[K].size() - 1; s >= 0; --s) {
                 auto& sg = L.stages[K][s];
                 {
                     int tok = prof_begin("dec_irc", st);
-                    irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+                    irc_stage_kernel<<<irc_stage_grid(hd, sg.m), grid3_threads(), 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
                                                                         sg.f[2].as<float2>(), sg.f[3].as<float2>(), 1,
                                                                         0);
                     prof_end(tok, st);
@@ -1259,10 +1256,9 @@ void scale_inverse_sum(DecPlan& D, int j, cudaStream_t st) {
         ha.S[K] = L.S[K].as<float2>();
         ha.V[K] = L.V[K].as<float>();
     }
-    long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
     {
         int tok = prof_begin("dec_herm_sum", st);
-        hermitian_sum_kernel<<<grid_for(tot), 256, 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
+        hermitian_sum_kernel<<<grid3_blocks(L.n[0], L.n[1], L.n[2]), grid3_threads(), 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
                                                              1.0f / 3.0f);
         prof_end(tok, st);
     }
@@ -1294,11 +1290,10 @@ void scale_forward_adjoint(DecPlan& D, int j, const float* c, int es, cudaStream
         }
         for (int m = 0; m < 3; ++m)
             if (m != K) block_fft(D, S, hd, m, L.bsize[K][m], false, st);
-        long long tot = (long long)hd[0] * hd[1] * hd[2];
         for (int sg_i = (int)L.stages[K].size() - 1; sg_i >= 0; --sg_i) {
             auto& sg = L.stages[K][sg_i];
             int tok = prof_begin("dec_irc", st);
-            irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+            irc_stage_kernel<<<irc_stage_grid(hd, sg.m), grid3_threads(), 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
                                                                 sg.f[0].as<float2>(), sg.f[1].as<float2>(), 1, 1);
             prof_end(tok, st);
             cuda_check(cudaGetLastError(), "irc_stage_kernel");
@@ -1309,9 +1304,8 @@ void scale_forward_adjoint(DecPlan& D, int j, const float* c, int es, cudaStream
         ha.S[K] = S;
         ha.V[K] = L.V[K].as<float>();
     }
-    long long tot = (long long)L.n[0] * L.n[1] * L.n[2];
     int tok = prof_begin("dec_hg_adjoint", st);
-    hg_adjoint_sum_kernel<<<grid_for(tot), 256, 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
+    hg_adjoint_sum_kernel<<<grid3_blocks(L.n[0], L.n[1], L.n[2]), grid3_threads(), 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
                                                           sK[0], sK[1], sK[2]);
     prof_end(tok, st);
     cuda_check(cudaGetLastError(), "hg_adjoint_sum_kernel");
@@ -1326,17 +1320,16 @@ void scale_inverse_adjoint(DecPlan& D, int j, float* c, int es, cudaStream_t st)
     for (int K = 0; K < 3; ++K) {
         const int* hd = L.hd[K];
         float2* S = L.S[K].as<float2>();
-        long long tot = (long long)hd[0] * hd[1] * hd[2];
         {
             int tok = prof_begin("dec_herm_gather", st);
-            herm_gather_kernel<<<grid_for(tot), 256, 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], S,
+            herm_gather_kernel<<<grid3_blocks(hd[0], hd[1], hd[2]), grid3_threads(), 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], S,
                                                                L.V[K].as<float>(), K, 1.0f / 3.0f);
             prof_end(tok, st);
             cuda_check(cudaGetLastError(), "herm_gather_kernel");
         }
         for (auto& sg : L.stages[K]) {
             int tok = prof_begin("dec_irc", st);
-            irc_stage_kernel<<<grid_for(tot / 2), 256, 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
+            irc_stage_kernel<<<irc_stage_grid(hd, sg.m), grid3_threads(), 0, st>>>(S, hd[0], hd[1], hd[2], K, sg.m, sg.b,
                                                                 sg.f[2].as<float2>(), sg.f[3].as<float2>(), 0, 1);
             prof_end(tok, st);
             cuda_check(cudaGetLastError(), "irc_stage_kernel");
