@@ -43,6 +43,8 @@ struct DecLevelDev {
     long long blk_elems[3];
     int nsub[3];
     DevMem S[3];                      // this level's half-K spectra S_K
+    DevMem inv[3];                    // box position along axis d of each spectrum index (-1 outside the box)
+    bool merge_fused = false;         // the box maps are one to one: the merge runs inside the Hermitian sum
 };
 
 struct DecPlan {
@@ -446,7 +448,19 @@ struct HermArgs {
     const float2* S[3];
     const float* V[3];
 };
-__global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs ha, float third) {
+// With MERGE, the pyramid merge of the level (pyr_merge_kernel) on the box
+// points in the same pass: X = sqrt(1-L^2) X + L D^1.5 low there, with the
+// same arithmetic, located by the inverse box maps.
+struct MergeArgs {
+    const int* inv[3];
+    const int* jl[3];
+    const float* lw;
+    const float* hw;
+    const float2* low;
+    int c0, c1, l0, l1;
+};
+template <bool MERGE>
+__global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs ha, float third, MergeArgs mg) {
     int n[3] = {n0, n1, n2};
     {
         int k[3];
@@ -464,6 +478,15 @@ __global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs
                 const int m0 = k[0] ? n0 - k[0] : 0, m1 = k[1] ? n1 - k[1] : 0, m2 = k[2] ? n2 - k[2] : 0;
                 long long a = lin3(m0, m1, m2, hd[0], hd[1]);
                 v = c_add(v, c_scale(c_conj(ha.S[K][a]), third * ha.V[K][a]));
+            }
+        }
+        if (MERGE) {
+            const int a = mg.inv[0][k[0]], b = mg.inv[1][k[1]], c = mg.inv[2][k[2]];
+            if ((a | b | c) >= 0) {
+                const long long qb = lin3(a, b, c, mg.c0, mg.c1);
+                const float2 h = c_scale(v, mg.hw[qb]);
+                const float2 w = c_scale(mg.low[lin3(mg.jl[0][a], mg.jl[1][b], mg.jl[2][c], mg.l0, mg.l1)], mg.lw[qb]);
+                v = c_add(h, w);
             }
         }
         X[q] = v;
@@ -662,6 +685,24 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
             upload_vec(L->idx_low[d], pl.idx_low[d]);
         }
         {
+            // inverse box maps: spectrum index -> box position, where every
+            // spectrum index is in the box at most once
+            bool one_to_one = true;
+            for (int d = 0; d < 3; ++d) {
+                std::vector<int> inv((size_t)L->n[d], -1);
+                for (int a = 0; a < L->cnt[d]; ++a) {
+                    const int i = pl.idx[d][a];
+                    if (i < 0 || i >= L->n[d] || inv[i] >= 0) {
+                        one_to_one = false;
+                        break;
+                    }
+                    inv[i] = a;
+                }
+                upload_vec(L->inv[d], inv);
+            }
+            L->merge_fused = one_to_one;
+        }
+        {
             // src/pyramid/fourier_pyramid.jl:221-240 (file numbering): the
             // separable lowpass L on the box, its D^-+1.5 scalings and
             // sqrt(1 - L^2), in float64.
@@ -812,6 +853,7 @@ Lines block_lines(const int hd[3], int m, int bl) {
     g.s2 = (long long)bl * str[m];
     g.si = str[m];
     g.nlines = hd[o[0]] * hd[o[1]] * (hd[m] / bl);
+    g.fast_div();
     return g;
 }
 
@@ -981,6 +1023,7 @@ Lines k_lines(const DecLevelDev& L, int K) {
     g.s1 = str[b];
     g.s2 = 0;
     g.si = str[K];
+    g.fast_div();
     return g;
 }
 
@@ -1248,21 +1291,41 @@ void scale_inverse(DecPlan& D, int j, const float* c, int es, cudaStream_t st) {
 }
 
 // Level j of the synthesis after the plane pass: the Hermitian sum of its
-// three hourglasses into the level spectrum.
-void scale_inverse_sum(DecPlan& D, int j, cudaStream_t st) {
+// three hourglasses into the level spectrum, then the pyramid merge with the
+// coarser spectrum (inside the same pass where the box maps are one to one).
+void scale_inverse_sum_merge(DecPlan& D, int j, cudaStream_t st) {
     DecLevelDev& L = *D.lv[j];
     HermArgs ha;
     for (int K = 0; K < 3; ++K) {
         ha.S[K] = L.S[K].as<float2>();
         ha.V[K] = L.V[K].as<float>();
     }
+    MergeArgs mg{};
+    if (L.merge_fused) {
+        for (int d = 0; d < 3; ++d) {
+            mg.inv[d] = L.inv[d].as<int>();
+            mg.jl[d] = L.idx_low[d].as<int>();
+        }
+        mg.lw = L.lw_merge.as<float>();
+        mg.hw = L.hw.as<float>();
+        mg.low = D.spectra[j + 1]->as<float2>();
+        mg.c0 = L.cnt[0];
+        mg.c1 = L.cnt[1];
+        mg.l0 = L.nlow[0];
+        mg.l1 = L.nlow[1];
+    }
     {
         int tok = prof_begin("dec_herm_sum", st);
-        hermitian_sum_kernel<<<grid3_blocks(L.n[0], L.n[1], L.n[2]), grid3_threads(), 0, st>>>(D.spectra[j]->as<float2>(), L.n[0], L.n[1], L.n[2], ha,
-                                                             1.0f / 3.0f);
+        const dim3 g = grid3_blocks(L.n[0], L.n[1], L.n[2]);
+        float2* X = D.spectra[j]->as<float2>();
+        if (L.merge_fused)
+            hermitian_sum_kernel<true><<<g, grid3_threads(), 0, st>>>(X, L.n[0], L.n[1], L.n[2], ha, 1.0f / 3.0f, mg);
+        else
+            hermitian_sum_kernel<false><<<g, grid3_threads(), 0, st>>>(X, L.n[0], L.n[1], L.n[2], ha, 1.0f / 3.0f, mg);
         prof_end(tok, st);
     }
     cuda_check(cudaGetLastError(), "hermitian_sum_kernel");
+    if (!L.merge_fused) pyr_merge(D, j, st);
 }
 
 // Adjoint of scale_forward: the subbands of level j (real, in c) to the
@@ -1386,10 +1449,7 @@ void dec_synthesize(DecPlan& D, const void* c, void* x, cudaStream_t st) {
         fft_real_full(D, cin, es, nl, D.spectra[D.J]->as<float2>(), st);
         for (int j = D.J - 1; j >= 0; --j) scale_inverse(D, j, cin, es, st);
         irc_plane_launch_levels<true>(D, st);
-        for (int j = D.J - 1; j >= 0; --j) {
-            scale_inverse_sum(D, j, st);
-            pyr_merge(D, j, st);
-        }
+        for (int j = D.J - 1; j >= 0; --j) scale_inverse_sum_merge(D, j, st);
         float scale = (float)(1.0 / ((double)D.dims[0] * D.dims[1] * D.dims[2]));
         ifft_full_real(D, D.spectra[0]->as<float2>(), D.dims, xout, es, scale, st);
     }

@@ -222,11 +222,24 @@ struct Lines {
     int nlines = 0;
     int B0 = 1, B1 = 1;
     long long s0 = 0, s1 = 0, s2 = 0, si = 0;
+    // ceil(2^32 / B0), ceil(2^32 / B1) where the line index splits by
+    // multiply-high division are exact (0: integer division).  l / B =
+    // umulhi(l, m) is exact when B is a power of two or l * B < 2^32
+    // (Granlund and Montgomery, "Division by invariant integers using
+    // multiplication", 1994); fast_div checks that for every l < nlines.
+    unsigned m0 = 0, m1 = 0;
+    __host__ void fast_div() {
+        const unsigned long long lim = 1ull << 32, n = (unsigned long long)nlines + 64;
+        m0 = m1 = 0;
+        if (B0 > 1 && n * (unsigned long long)B0 < lim) m0 = 0xFFFFFFFFu / (unsigned)B0 + 1u;
+        if (B1 > 1 && (n / (unsigned long long)B0 + 1) * (unsigned long long)B1 < lim)
+            m1 = 0xFFFFFFFFu / (unsigned)B1 + 1u;
+    }
     __device__ __forceinline__ long long base(int l) const {
-        int l0 = l % B0;
-        int r = l / B0;
-        int l1 = r % B1;
-        int l2 = r / B1;
+        const int r = B0 == 1 ? l : (m0 ? (int)__umulhi((unsigned)l, m0) : l / B0);
+        const int l0 = l - r * B0;
+        const int l2 = B1 == 1 ? r : (m1 ? (int)__umulhi((unsigned)r, m1) : r / B1);
+        const int l1 = r - l2 * B1;
         return (long long)l0 * s0 + (long long)l1 * s1 + (long long)l2 * s2;
     }
 };

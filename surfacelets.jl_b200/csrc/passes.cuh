@@ -318,6 +318,7 @@ inline Lines axis_lines(const int d[3], int a) {
     g.s1 = s[o1];
     g.s2 = 0;
     g.si = s[a];
+    g.fast_div();
     return g;
 }
 
