@@ -274,7 +274,7 @@ int sfl_stream_synthesize_end(sfl_plan* plan, void* x, void* stream);
  * plan size at start-up too: the first call on a device looks up the
  * scratch's device address (cudaGetSymbolAddress), and under lazy module
  * loading a kernel's first launch loads its code; both belong before the
- * allocation-free phase and before any stream capture.  The address is
+ * allocation-free phase.  The address is
  * cached per device for the process; do not call this again on a device
  * after cudaDeviceReset.  Limits: real plans only, and (n1/2+1)*n2*n3 <=
  * 262144 (e.g. 64^3); larger sizes return SFL_ERR_ARGUMENT.  All calls share

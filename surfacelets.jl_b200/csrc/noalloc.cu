@@ -17,7 +17,7 @@
 // (cudaGetSymbolAddress), and under CUDA's lazy module loading the first
 // launch of a kernel loads its code, which can take device memory; so the
 // first call for each plan size belongs at start-up, before the
-// allocation-free phase and before any stream capture.  The cached address
+// allocation-free phase.  The cached address
 // is per device and per process: after cudaDeviceReset the library's module
 // is loaded anew and the cache is stale, so a process that resets a device
 // must not call this entry point on it again.
