@@ -45,7 +45,7 @@ extern "C" {
 #define SFL_ERR_CUDA (-3)        /* a CUDA call failed */
 #define SFL_ERR_ALLOC (-4)       /* device memory could not be allocated */
 #define SFL_ERR_STATE (-5)       /* call out of order (streaming) */
-#define SFL_ERR_UNSUPPORTED (-6) /* a size or option this build does not handle */
+#define SFL_ERR_UNSUPPORTED (-6) /* a size or option this library does not handle */
 #define SFL_ERR_TIMEOUT (-7)     /* a bounded device wait of an earlier call on the plan ran out */
 
 #define SFL_MAX_SCALES 16

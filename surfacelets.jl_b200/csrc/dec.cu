@@ -665,7 +665,7 @@ static void upload_vec(DevMem& m, const std::vector<T>& v) {
 
 void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], int dtype) {
     for (int d = 0; d < 3; ++d)
-        if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
+        if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this library");
     std::unique_ptr<DecPlan> D(new DecPlan);
     D->design = surf_design(p, dims, false);   // factors only: the tables are composed on the device
     const SurfDesign& S = D->design;

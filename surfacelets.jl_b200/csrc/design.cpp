@@ -174,14 +174,14 @@ std::vector<double> rcos_axis(int n, Rat w, Rat t, int& P) {
 void ns_check_params(const sfl_ns_params& p) {
     if (p.scales < 1) throw ArgError("scales must be ≥ 1, got " + std::to_string(p.scales));
     if (p.scales > SFL_MAX_SCALES)
-        throw ArgError("scales must be ≤ " + std::to_string(SFL_MAX_SCALES) + " in this build, got " +
+        throw ArgError("scales must be ≤ " + std::to_string(SFL_MAX_SCALES) + " in this library, got " +
                        std::to_string(p.scales));
     for (int j = 0; j < p.scales; ++j)
         if (p.direction_levels[j] < 0)
             throw ArgError("direction_levels entries must be ≥ 0, got " + fmt_vec(p.direction_levels, p.scales));
     for (int j = 0; j < p.scales; ++j)
         if (p.direction_levels[j] > 12)
-            throw ArgError("direction_levels entries must be ≤ 12 in this build, got " +
+            throw ArgError("direction_levels entries must be ≤ 12 in this library, got " +
                            fmt_vec(p.direction_levels, p.scales));
     if (p.bernstein_order < 1)
         throw ArgError("bernstein_order must be ≥ 1, got " + std::to_string(p.bernstein_order));
@@ -507,7 +507,7 @@ static const std::vector<double>& cbd_ladder(int bo) {
 void surf_check_params(const sfl_surf_params& p) {
     if (p.scales < 1) throw ArgError("scales must be ≥ 1, got " + std::to_string(p.scales));
     if (p.scales > SFL_MAX_SCALES)
-        throw ArgError("scales must be ≤ " + std::to_string(SFL_MAX_SCALES) + " in this build, got " +
+        throw ArgError("scales must be ≤ " + std::to_string(SFL_MAX_SCALES) + " in this library, got " +
                        std::to_string(p.scales));
     for (int j = 0; j < p.scales; ++j)
         for (int K = 0; K < 3; ++K)
@@ -517,7 +517,7 @@ void surf_check_params(const sfl_surf_params& p) {
         for (int K = 0; K < 3; ++K)
             for (int m = 0; m < 3; ++m)
                 if (m != K && p.levels[j][K][m] > 12)
-                    throw ArgError("directional levels must be ≤ 12 in this build");
+                    throw ArgError("directional levels must be ≤ 12 in this library");
     Rat w[2], t[2], D[2];
     surf_pyramid_mode(p.pyramid_ratio, w, t, D);
     cbd_ladder(p.checkerboard_order);

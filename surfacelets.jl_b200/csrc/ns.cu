@@ -248,7 +248,7 @@ static std::vector<float> to_f32(const std::vector<double>& v) {
 // with the hourglass masks alone as group factors, no pyramid and no lowpass.
 void ns_plan_init(NSPlan& P, const sfl_ns_params& p, const int dims[3], int dtype, bool ndfb) {
     for (int d = 0; d < 3; ++d)
-        if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this build");
+        if (dims[d] > 8192) throw ArgError("axis lengths above 8192 are not supported by this library");
     P.ndfb = ndfb;
     P.design = ns_design(p, dims, !ndfb, false);
     const NSDesign& D = P.design;
@@ -514,7 +514,7 @@ void accum_items(NSPlan& P, int i0, int nz, bool analysis_masks, float2* acc, fl
     }
     int T = pass_tile(n);
     while (T > 1 && T * n > kAccMax * 256) --T;
-    if (T * n > kAccMax * 256) throw ArgError("axis 3 is too long for the accumulating pass of this build");
+    if (T * n > kAccMax * 256) throw ArgError("axis 3 is too long for the accumulating pass of this library");
     int npad = n + 1;
     size_t smem = pass_smem_bytes(n, T);
     static bool configured = false;
