@@ -207,7 +207,9 @@ int sfl_plan_set_pipeline(sfl_plan* plan, int32_t pipeline);
 int sfl_plan_tuning(const sfl_plan* plan, int32_t* pipeline, int32_t* group);
 
 /* The tile of the slab pipeline's axis-3 analysis pass: subbands a CTA takes
- * (1, 2, 4 or 8; 0 = the default, 8 or the SFL_MASK_IPC environment variable).
+ * (1, 2, 4 or 8; 0 = the default: the SFL_MASK_IPC environment variable if
+ * set, else 8, halved per launch while the launch holds fewer CTAs than the
+ * GPU has SMs).  A tile set here is used as given.
  * set != 0 writes *ipc, else reads it.  The autotuner picks it after the
  * pipeline and group.  NS plans only.  No counterpart in the reference. */
 int sfl_plan_tile(sfl_plan* plan, int32_t set, int32_t* ipc);

@@ -1218,6 +1218,12 @@ int sfl_batch_create(int32_t n, sfl_plan* const* plans, const int32_t* ops, cons
                 for (auto& x : s) sfl::cuda_check(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "stream");
                 sfl::cuda_check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
                 for (auto& e : join) sfl::cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+                // the graph's branches run concurrently: launch shapes for that (the eager pass too, so that it
+                // configures the kernels the capture records)
+                struct Concurrent {
+                    explicit Concurrent(bool on) { sfl::ns_set_concurrent(on); }
+                    ~Concurrent() { sfl::ns_set_concurrent(false); }
+                } concurrent(distinct.size() > 1);
                 // one eager pass: validates the arguments and configures every kernel outside the capture
                 for (int i = 0; i < n; ++i) run_op(plans[i], ops[i], inputs[i], outputs[i], s[0]);
                 sfl::cuda_check(cudaStreamSynchronize(s[0]), "batch warm-up");

@@ -984,27 +984,37 @@ void launch_mask_group_ipc(const NSPlan& P, const float2* X, float2* Y, int nz, 
     cuda_check(cudaGetLastError(), "ns_slab_mask_group_kernel launch");
 }
 
-// Subbands a CTA of the analysis line pass takes: the line's X and group
-// factor are loaded once for all of them.
-// Subbands a CTA of the analysis axis-3 pass: the plan's choice (the
-// autotuner's tile), else up to 8 (a finest-scale group of [2,2,3] in one
-// CTA: 2027 vs 2013 Mvox/s for 4 on the bench workload), or at most
-// SFL_MASK_IPC (1, 2, 4 or 8) from the environment, read once.
-int mask_ipc(const NSPlan& P, int nz) {
+thread_local bool t_concurrent = false;
+
+// Subbands a CTA of the analysis axis-3 pass (the line's X and group factor
+// are loaded once for all of them).  An explicit choice is taken as given:
+// the plan's (the autotuner's tile), else SFL_MASK_IPC (1, 2, 4 or 8) from
+// the environment, read once.  By default up to 8 (a finest-scale group of
+// [2,2,3] in one CTA: 2027 vs 2013 Mvox/s for 4 on the bench workload),
+// and for launches that run alone halved while the launch would hold fewer
+// CTAs than the GPU has SMs (the small boxes of coarse scales: 30 line blocks
+// at 128^3 [2,2,3] scale 1): the pass 3.32 -> 2.93 ms a step of eight volumes
+// as plain calls, but 2038 -> 2031 Mvox/s in the four-branch graph, where the
+// other branches fill the GPU and the split CTAs only reload X.
+int mask_ipc(const NSPlan& P, int nz, int nblocks) {
     static const int env_cap = [] {
         const char* e = std::getenv("SFL_MASK_IPC");
-        const int v = e ? std::atoi(e) : 8;
+        if (!e) return 0;
+        const int v = std::atoi(e);
         return v >= 8 ? 8 : (v >= 4 ? 4 : (v >= 2 ? 2 : 1));
     }();
-    const int cap = P.ipc > 0 ? P.ipc : env_cap;
+    const int cap = P.ipc > 0 ? P.ipc : (env_cap > 0 ? env_cap : 8);
     const int m = std::min(nz, cap);
-    return m >= 8 ? 8 : (m >= 4 ? 4 : (m >= 2 ? 2 : 1));
+    int ipc = m >= 8 ? 8 : (m >= 4 ? 4 : (m >= 2 ? 2 : 1));
+    if (P.ipc <= 0 && env_cap == 0 && !t_concurrent)
+        while (ipc > 1 && (long long)nblocks * ((nz + ipc - 1) / ipc) < P.sms) ipc /= 2;
+    return ipc;
 }
 
 template <int N>
 void launch_mask_group(const NSPlan& P, const float2* X, float2* Y, int nz, const BoxMap& bx, int i0, int synth,
                        int nlines, int nch, long long xchs, long long ychs, int nbq, cudaStream_t st) {
-    switch (mask_ipc(P, nz)) {
+    switch (mask_ipc(P, nz, (nlines + RegGeom<N>::LP - 1) / RegGeom<N>::LP)) {
         case 8: launch_mask_group_ipc<N, 8>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
         case 4: launch_mask_group_ipc<N, 4>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
         case 2: launch_mask_group_ipc<N, 2>(P, X, Y, nz, bx, i0, synth, nlines, nch, xchs, ychs, nbq, st); return;
@@ -1197,6 +1207,8 @@ int chunk_end(const NSPlan& P, int i0) {
 }
 
 }  // namespace
+
+void ns_set_concurrent(bool on) { t_concurrent = on; }
 
 bool ns_slab_supported(int n1, int n2, int n3) {
     if (!reg_fft_supported(n3)) return false;

@@ -127,7 +127,7 @@ struct NSPlan {
     int nch = 1;          // 1 real, 2 complex
     bool ndfb = false;    // the standalone directional bank (no pyramid, no lowpass)
     int group = 8;
-    int ipc = 0;          // subbands a CTA of the slab axis-3 analysis pass takes (1, 2, 4; 0: 4, or SFL_MASK_IPC)
+    int ipc = 0;          // subbands a CTA of the slab axis-3 analysis pass takes (1, 2, 4, 8; 0: the default, mask_ipc)
     std::vector<NSItem> items_host;   // streaming / item order: directional ascending, then lowpass
     DevMem items;
     DevMem G, Bl, vec, planes;
@@ -184,6 +184,10 @@ void ns_stream_synth_end(NSPlan& P, void* x, cudaStream_t st);
 void ns_design_tables_device(NSPlan& P);
 // Slab pipeline (ns_slab.cu).
 bool ns_slab_supported(int n1, int n2, int n3);
+// Launches from this thread run beside others on concurrent streams (a batch
+// graph being captured): the slab pipeline's launch shapes then favour fewer,
+// larger CTAs over filling the GPU alone.
+void ns_set_concurrent(bool on);
 void ns_use_slabs(NSPlan& P);
 NSBox ns_make_box(int nk1, int b2, int n2);
 NSBox ns_table_box(const std::vector<double>& g, int h1, int n2, int n3);
