@@ -47,6 +47,27 @@ struct DecLevelDev {
     bool merge_fused = false;         // the box maps are one to one: the merge runs inside the Hermitian sum
 };
 
+// Two side streams and the events that fork them from, and join them back
+// to, the caller's stream: the per-level passes of a call, which touch only
+// their own level's buffers and coefficients, run on them concurrently (the
+// fork-join pattern that stream capture records as graph branches).
+struct LevelStreams {
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    void create() {
+        for (auto& x : side) cuda_check(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "cudaEventCreate");
+        for (auto& e : join) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    ~LevelStreams() {
+        for (auto& e : join)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        for (auto& x : side)
+            if (x) cudaStreamDestroy(x);
+    }
+};
+
 struct DecPlan {
     SurfDesign design;
     int dims[3];
@@ -56,6 +77,7 @@ struct DecPlan {
     std::vector<std::unique_ptr<DecLevelDev>> lv;
     std::vector<std::unique_ptr<DevMem>> spectra;   // J + 1 full complex grids
     std::map<int, std::unique_ptr<FFTLen>> ffts;
+    LevelStreams ls;
 };
 
 void DecPlanDeleter::operator()(DecPlan* d) const { delete d; }
@@ -771,6 +793,7 @@ void dec_plan_create(Plan& plan, const sfl_surf_params& p, const int dims[3], in
             const int* h = L->hd[K];
             L->S[K].alloc(sizeof(float2) * (size_t)h[0] * h[1] * h[2]);
         }
+    D->ls.create();
     plan.dec.reset(D.release());
 }
 
@@ -1412,6 +1435,26 @@ void scale_inverse_adjoint(DecPlan& D, int j, float* c, int es, cudaStream_t st)
     }
 }
 
+// f(j, stream) for the levels j = 0 .. J-1, level 0 on st and the others on
+// the plan's side streams, all after the work already on st; st waits for
+// all of them.
+template <class F>
+void per_level(DecPlan& D, cudaStream_t st, F f) {
+    if (D.J < 2) {
+        for (int j = 0; j < D.J; ++j) f(j, st);
+        return;
+    }
+    LevelStreams& ls = D.ls;
+    cuda_check(cudaEventRecord(ls.fork, st), "cudaEventRecord");
+    const int nside = std::min(D.J - 1, 2);
+    for (int k = 0; k < nside; ++k) cuda_check(cudaStreamWaitEvent(ls.side[k], ls.fork, 0), "cudaStreamWaitEvent");
+    for (int j = 0; j < D.J; ++j) f(j, j == 0 ? st : ls.side[(j - 1) % 2]);
+    for (int k = 0; k < nside; ++k) {
+        cuda_check(cudaEventRecord(ls.join[k], ls.side[k]), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(st, ls.join[k], 0), "cudaStreamWaitEvent");
+    }
+}
+
 void cscale(float2* X, long long n, float s, cudaStream_t st) {
     int tok = prof_begin("dec_scale", st);
     cscale_kernel<<<grid_for(n), 256, 0, st>>>(X, n, s);
@@ -1432,10 +1475,13 @@ void dec_analyze(DecPlan& D, const void* x, void* c, cudaStream_t st) {
         // that one plane pass covers the hourglasses of all levels
         for (int j = 0; j < D.J; ++j) pyr_split(D, j, st);
         irc_plane_launch_levels<false>(D, st);
-        for (int j = 0; j < D.J; ++j) scale_forward(D, j, cout, es, st);
+        // the levels' block FFTs and C2R, and the lowpass (after the coarsest level), concurrently
         const int* nl = S.pyramid[D.J - 1].nlow;
-        float scale = (float)(1.0 / ((double)nl[0] * nl[1] * nl[2]));
-        ifft_full_real(D, D.spectra[D.J]->as<float2>(), nl, cout, es, scale, st);
+        const float scale = (float)(1.0 / ((double)nl[0] * nl[1] * nl[2]));
+        per_level(D, st, [&](int j, cudaStream_t s) {
+            scale_forward(D, j, cout, es, s);
+            if (j == D.J - 1) ifft_full_real(D, D.spectra[D.J]->as<float2>(), nl, cout, es, scale, s);
+        });
     }
 }
 
@@ -1446,8 +1492,11 @@ void dec_synthesize(DecPlan& D, const void* c, void* x, cudaStream_t st) {
         const float* cin = reinterpret_cast<const float*>(c) + ch;
         float* xout = reinterpret_cast<float*>(x) + ch;
         const int* nl = S.pyramid[D.J - 1].nlow;
-        fft_real_full(D, cin, es, nl, D.spectra[D.J]->as<float2>(), st);
-        for (int j = D.J - 1; j >= 0; --j) scale_inverse(D, j, cin, es, st);
+        // the levels' R2C and block FFTs, and the lowpass FFT (before the coarsest level), concurrently
+        per_level(D, st, [&](int j, cudaStream_t s) {
+            if (j == D.J - 1) fft_real_full(D, cin, es, nl, D.spectra[D.J]->as<float2>(), s);
+            scale_inverse(D, j, cin, es, s);
+        });
         irc_plane_launch_levels<true>(D, st);
         for (int j = D.J - 1; j >= 0; --j) scale_inverse_sum_merge(D, j, st);
         float scale = (float)(1.0 / ((double)D.dims[0] * D.dims[1] * D.dims[2]));
