@@ -495,11 +495,11 @@ __global__ void hermitian_sum_kernel(float2* X, int n0, int n1, int n2, HermArgs
             hd[K] = n[K] / 2 + 1;
             if (k[K] < hd[K]) {
                 long long a = lin3(k[0], k[1], k[2], hd[0], hd[1]);
-                v = c_add(v, c_scale(ha.S[K][a], third * ha.V[K][a]));
+                v = c_fma(ha.S[K][a], third * ha.V[K][a], v);
             } else {
                 const int m0 = k[0] ? n0 - k[0] : 0, m1 = k[1] ? n1 - k[1] : 0, m2 = k[2] ? n2 - k[2] : 0;
                 long long a = lin3(m0, m1, m2, hd[0], hd[1]);
-                v = c_add(v, c_scale(c_conj(ha.S[K][a]), third * ha.V[K][a]));
+                v = c_fma(c_conj(ha.S[K][a]), third * ha.V[K][a], v);
             }
         }
         if (MERGE) {
@@ -531,7 +531,7 @@ __global__ void hg_adjoint_sum_kernel(float2* X, int n0, int n1, int n2, HermArg
             hd[K] = n[K] / 2 + 1;
             if (k[K] < hd[K]) {
                 long long a = lin3(k[0], k[1], k[2], hd[0], hd[1]);
-                v = c_add(v, c_scale(ha.S[K][a], sK[K] * ha.V[K][a]));
+                v = c_fma(ha.S[K][a], sK[K] * ha.V[K][a], v);
             }
         }
         X[q] = v;

@@ -22,12 +22,22 @@ struct FFTShape {
     const float2* tw = nullptr;   // device: n entries, e^{-2 pi i t / n}
 };
 
+// Complex arithmetic on (re, im) register pairs.  Additions, subtractions and
+// real scalings use sm_100's paired FP32 instructions (__fadd2_rn,
+// __fmul2_rn, __ffma2_rn: one instruction for both components, each rounded
+// as its scalar form), which halves the issue slots of the butterflies'
+// additions.  The complex product keeps scalar FMUL / FFMA: its cross terms
+// pair a component with the other operand's opposite component.
 __device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 c_scale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+// acc + a s, one rounding a component
+__device__ __forceinline__ float2 c_fma(float2 a, float s, float2 acc) {
+    return __ffma2_rn(a, make_float2(s, s), acc);
+}
 __device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
 // Kahan step s += v with compensation c (Kahan 1965), per component:
 // y = v - c; t = s + y; c = (t - s) - y; s = t.  The explicit round-to-nearest
@@ -61,10 +71,11 @@ struct Dft<3> {
         const float c = -0.5f;
         const float s = inv ? -0.86602540378443864676f : 0.86602540378443864676f;
         float2 t1 = c_add(v[1], v[2]);
-        float2 t2 = c_sub(v[1], v[2]);
-        float2 m = make_float2(v[0].x + c * t1.x, v[0].y + c * t1.y);
-        // -i s t2
-        float2 r = make_float2(s * t2.y, -s * t2.x);
+        // -i (v1 - v2), formed rotated by scalar subtractions
+        float2 t2 = make_float2(v[1].y - v[2].y, v[2].x - v[1].x);
+        float2 m = c_fma(t1, c, v[0]);
+        // -i s (v1 - v2)
+        float2 r = c_scale(t2, s);
         v[0] = c_add(v[0], t1);
         v[1] = c_add(m, r);
         v[2] = c_sub(m, r);
@@ -77,7 +88,9 @@ struct Dft<4> {
         float2 t0 = c_add(v[0], v[2]);
         float2 t1 = c_sub(v[0], v[2]);
         float2 t2 = c_add(v[1], v[3]);
-        float2 t3 = c_rot(c_sub(v[1], v[3]), inv);
+        // -+i (v1 - v3), formed rotated by scalar subtractions
+        float2 t3 = inv ? make_float2(v[3].y - v[1].y, v[1].x - v[3].x)
+                        : make_float2(v[1].y - v[3].y, v[3].x - v[1].x);
         v[0] = c_add(t0, t2);
         v[2] = c_sub(t0, t2);
         v[1] = c_add(t1, t3);
@@ -92,18 +105,21 @@ struct Dft<5> {
         const float c2 = -0.80901699437494742410f;   // cos(4pi/5)
         const float s1 = inv ? -0.95105651629515357212f : 0.95105651629515357212f;   // sin(2pi/5)
         const float s2 = inv ? -0.58778525229247312917f : 0.58778525229247312917f;   // sin(4pi/5)
-        float2 a14 = c_add(v[1], v[4]), d14 = c_sub(v[1], v[4]);
-        float2 a23 = c_add(v[2], v[3]), d23 = c_sub(v[2], v[3]);
-        float2 m1 = make_float2(v[0].x + c1 * a14.x + c2 * a23.x, v[0].y + c1 * a14.y + c2 * a23.y);
-        float2 m2 = make_float2(v[0].x + c2 * a14.x + c1 * a23.x, v[0].y + c2 * a14.y + c1 * a23.y);
-        // r1 = s1 d14 + s2 d23 ; r2 = s2 d14 - s1 d23 ; X1 = m1 - i r1 ; X2 = m2 - i r2
-        float2 r1 = make_float2(s1 * d14.x + s2 * d23.x, s1 * d14.y + s2 * d23.y);
-        float2 r2 = make_float2(s2 * d14.x - s1 * d23.x, s2 * d14.y - s1 * d23.y);
-        v[0] = make_float2(v[0].x + a14.x + a23.x, v[0].y + a14.y + a23.y);
-        v[1] = make_float2(m1.x + r1.y, m1.y - r1.x);
-        v[4] = make_float2(m1.x - r1.y, m1.y + r1.x);
-        v[2] = make_float2(m2.x + r2.y, m2.y - r2.x);
-        v[3] = make_float2(m2.x - r2.y, m2.y + r2.x);
+        float2 a14 = c_add(v[1], v[4]);
+        float2 a23 = c_add(v[2], v[3]);
+        // -i d14 and -i d23, formed rotated by scalar subtractions
+        float2 e14 = make_float2(v[1].y - v[4].y, v[4].x - v[1].x);
+        float2 e23 = make_float2(v[2].y - v[3].y, v[3].x - v[2].x);
+        float2 m1 = c_fma(a23, c2, c_fma(a14, c1, v[0]));
+        float2 m2 = c_fma(a23, c1, c_fma(a14, c2, v[0]));
+        // -i r1 = s1 e14 + s2 e23 ; -i r2 = s2 e14 - s1 e23 ; X1 = m1 - i r1 ; X2 = m2 - i r2
+        float2 q1 = c_fma(e23, s2, c_scale(e14, s1));
+        float2 q2 = c_fma(e23, -s1, c_scale(e14, s2));
+        v[0] = c_add(c_add(v[0], a14), a23);
+        v[1] = c_add(m1, q1);
+        v[4] = c_sub(m1, q1);
+        v[2] = c_add(m2, q2);
+        v[3] = c_sub(m2, q2);
     }
 };
 
@@ -116,11 +132,11 @@ struct Dft<8> {
         Dft<4>::run(o, inv);
         const float h = 0.70710678118654752440f;
         // w8^1 = h(1 -+ i), w8^2 = -+i, w8^3 = h(-1 -+ i)
-        float2 o1 = inv ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
-                        : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+        float2 o1 = c_scale(inv ? make_float2(o[1].x - o[1].y, o[1].x + o[1].y)
+                                : make_float2(o[1].x + o[1].y, o[1].y - o[1].x), h);
         float2 o2 = c_rot(o[2], inv);
-        float2 o3 = inv ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
-                        : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+        float2 o3 = c_scale(inv ? make_float2(-(o[3].x + o[3].y), o[3].x - o[3].y)
+                                : make_float2(o[3].y - o[3].x, -(o[3].x + o[3].y)), h);
         v[0] = c_add(e[0], o[0]);
         v[4] = c_sub(e[0], o[0]);
         v[1] = c_add(e[1], o1);

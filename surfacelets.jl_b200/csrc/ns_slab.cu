@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
                 const float g = gf[j * N2 + k];
                 const float m = !wedges ? g : (before ? g * mk.wb[k3 * mk.wbs] : g * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]));
                 float2& tsum = sum(j * N2 + k);
-                tsum = c_add(tsum, c_scale(u[j * N2 + k], m));
+                tsum = c_fma(u[j * N2 + k], m, tsum);
             }
         __syncthreads();   // the exchange rows are reused by the next term
     }
