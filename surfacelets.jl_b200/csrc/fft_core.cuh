@@ -43,10 +43,10 @@ __device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.
 // y = v - c; t = s + y; c = (t - s) - y; s = t.  The explicit round-to-nearest
 // intrinsics keep the compiler from contracting or reordering it.
 __device__ __forceinline__ void kahan_add(float2& s, float2& c, float2 v) {
-    const float yx = __fsub_rn(v.x, c.x), yy = __fsub_rn(v.y, c.y);
-    const float tx = __fadd_rn(s.x, yx), ty = __fadd_rn(s.y, yy);
-    c = make_float2(__fsub_rn(__fsub_rn(tx, s.x), yx), __fsub_rn(__fsub_rn(ty, s.y), yy));
-    s = make_float2(tx, ty);
+    const float2 y = c_sub(v, c);
+    const float2 t = c_add(s, y);
+    c = c_sub(c_sub(t, s), y);
+    s = t;
 }
 // multiply by -i (forward) or +i (inverse)
 __device__ __forceinline__ float2 c_rot(float2 a, bool inv) {

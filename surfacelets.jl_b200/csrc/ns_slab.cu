@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
 #pragma unroll
                 for (int r = 0; r < N1; ++r)
                     v[r] = pp == 0 ? c_scale(cur[r], az)
-                                   : make_float2(fmaf(cur[r].x, az, v[r].x), fmaf(cur[r].y, az, v[r].y));
+                                   : c_fma(cur[r], az, v[r]);
             } else {
                 if (pp > 0) {
                     const float2* yz = yl + z * ystride;
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
 #pragma unroll
                 for (int r = 0; r < N1; ++r)
                     v[r] = pp == 0 ? c_scale(yb[r], az)
-                                   : make_float2(fmaf(yb[r].x, az, v[r].x), fmaf(yb[r].y, az, v[r].y));
+                                   : c_fma(yb[r], az, v[r]);
             }
         }
         float2 u[E];
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(256, accum_minb<N>()) ns_slab_accum_kernel(con
                 const float g = gf[j * N2 + k];
                 const float m = !wedges ? g : (before ? g * mk.wb[k3 * mk.wbs] : g * (mk.wa[k3 * mk.was] * mk.wb[k3 * mk.wbs]));
                 float2& tsum = sum(j * N2 + k);
-                tsum = c_fma(u[j * N2 + k], m, tsum);
+                tsum = make_float2(fmaf(u[j * N2 + k].x, m, tsum.x), fmaf(u[j * N2 + k].y, m, tsum.y));
             }
         __syncthreads();   // the exchange rows are reused by the next term
     }
@@ -475,15 +475,30 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
     uint64_t* bar = slab_bar<NA, NB>(sm);
     uint32_t phase = 0;
     slab_bar_init(bar);
+    const int per = a.nzc * a.n3;
+    auto slab_src = [&](int unit) {
+        const int ch = unit / per, ur = unit - ch * per;
+        const int z = ur / a.n3, s3 = ur - z * a.n3;
+        return a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
+    };
+    const uint32_t colbytes = (uint32_t)(((nk1 + 1) & ~1) * sizeof(float2));
+    bool requested = false;   // the unit's box was requested during the previous unit's C2R
     for (int u = blockIdx.x; u < a.units; u += gridDim.x) {
-        const int per = a.nzc * a.n3;
         const int ch = u / per, ur = u - ch * per;
         const int z = ur / a.n3, s3 = ur - z * a.n3;
-        const float2* src = a.spec + ch * a.spec_chstride + z * a.spec_zstride + (long long)s3 * SL;
         // the output slab (its offset may come from the item table: loaded ahead of the phases)
         float* out = a.vol + ch + a.vz.off(z) + (long long)s3 * PLANE * ES;
         // 1. the box of the slab into shared memory
-        slab_bulk_load<NB, P1>(S, src, nk1, nk2, b2, bar, phase, a.status);
+        if (!requested) {
+            slab_bulk_load<NB, P1>(S, slab_src(u), nk1, nk2, b2, bar, phase, a.status);
+        } else {
+            mbar_wait_bounded(bar, phase, a.status);
+            phase ^= 1;
+        }
+        // the next unit of this CTA, whose box columns are requested as soon as their pair is transformed
+        const int un = u + gridDim.x;
+        requested = un < a.units;
+        const float2* srcn = requested ? slab_src(un) : nullptr;
         // 2. inverse FFT along axis 2 of the rows k1 < nk1; columns outside the box are zero
         {
             const int p = lane & (LB::N2 - 1), s = lane / LB::N2;
@@ -536,6 +551,17 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
                     v[r] = 2 * i <= NA ? make_float2(A.x - B.y, A.y + B.x) : make_float2(A.x + B.y, B.x - A.y);
                 }
                 warp_line_fft<NA, true, 1>(v, p, valid, twA, ca);
+                if (requested) {
+                    // the warp's columns are free (the exchange ended with a warp barrier): lane c of the
+                    // first 2 LPW requests column 2 (base + warp LPW) + c of the next unit, if in its box
+                    fence_proxy_async();
+                    __syncwarp();
+                    const int k2 = 2 * (base + warp * LA::LPW) + lane;
+                    if (lane < 2 * LA::LPW && k2 < NB && (k2 <= b2 || k2 >= k2hi)) {
+                        mbar_expect_tx(bar, colbytes);
+                        bulk_load(S + P1 * k2, srcn + P1 * k2, colbytes, bar);
+                    }
+                }
                 if (valid) {
                     float* oa = out + (long long)(2 * l) * NA * ES;
                     float* ob = oa + (long long)NA * ES;
@@ -552,6 +578,8 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
             }
         }
         __syncthreads();   // the slab buffer is reused by the next unit
+        // every copy of the next unit is issued and announced: the one arrival of the barrier's phase
+        if (requested && threadIdx.x == 0) mbar_arrive(bar);
     }
 }
 
