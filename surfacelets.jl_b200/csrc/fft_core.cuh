@@ -39,6 +39,15 @@ __device__ __forceinline__ float2 c_fma(float2 a, float s, float2 acc) {
     return __ffma2_rn(a, make_float2(s, s), acc);
 }
 __device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+// The half spectra of two real lines a, b transformed as one complex line
+// z = a + i b, from zk = Z[k] and zn = Z[n - k]: A[k] = (zk + conj(zn)) / 2
+// and B[k] = (zk - conj(zn)) / (2 i).
+__device__ __forceinline__ float2 half_spec_a(float2 zk, float2 zn) {
+    return c_scale(__ffma2_rn(zn, make_float2(1.f, -1.f), zk), 0.5f);
+}
+__device__ __forceinline__ float2 half_spec_b(float2 zk, float2 zn) {
+    return c_scale(make_float2(zk.y + zn.y, zn.x - zk.x), 0.5f);
+}
 // Kahan step s += v with compensation c (Kahan 1965), per component:
 // y = v - c; t = s + y; c = (t - s) - y; s = t.  The explicit round-to-nearest
 // intrinsics keep the compiler from contracting or reordering it.

@@ -165,8 +165,8 @@ __device__ __forceinline__ void unpack_pair(const float2* xs, float2* S0, float2
         if (valid && k < nk1) {
             const float2 zk = xs[k];
             const float2 zn = xs[k == 0 ? 0 : NA - k];
-            ha[q] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-            hb[q] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+            ha[q] = half_spec_a(zk, zn);
+            hb[q] = half_spec_b(zk, zn);
         }
     }
     if (valid) {
@@ -254,8 +254,9 @@ __global__ void __launch_bounds__(kSlabThreads, 1) ns_slab_cluster_inv_kernel(Sl
 #pragma unroll
                         for (int k = 0; k < LA::N2; ++k) {
                             const int i1 = (p + LA::N2 * j) + LA::N1 * k;
-                            oa[i1 * ES] = v[j * LA::N2 + k].x * sc;
-                            ob[i1 * ES] = v[j * LA::N2 + k].y * sc;
+                            const float2 w = c_scale(v[j * LA::N2 + k], sc);
+                            oa[i1 * ES] = w.x;
+                            ob[i1 * ES] = w.y;
                         }
                 }
             }

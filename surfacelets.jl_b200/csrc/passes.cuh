@@ -160,8 +160,8 @@ struct StoreHalfPair {
             float2 zk = tile[t * npad + k];
             float2 zm_ = tile[t * npad + (k == 0 ? 0 : n - k)];
             // A = (Z[k] + conj(Z[-k]))/2 ; B = (Z[k] - conj(Z[-k]))/(2i)
-            float2 A = make_float2(0.5f * (zk.x + zm_.x), 0.5f * (zk.y - zm_.y));
-            float2 B = make_float2(0.5f * (zk.y + zm_.y), -0.5f * (zk.x - zm_.x));
+            float2 A = half_spec_a(zk, zm_);
+            float2 B = half_spec_b(zk, zm_);
             if (k != 0 && 2 * k != n) {
                 A = c_scale(A, wpair);
                 B = c_scale(B, wpair);
@@ -193,8 +193,8 @@ struct StoreFullPair {
             int la = 2 * (l0 + t);
             float2 zk = tile[t * npad + k];
             float2 zm_ = tile[t * npad + (k == 0 ? 0 : n - k)];
-            float2 A = make_float2(0.5f * (zk.x + zm_.x), 0.5f * (zk.y - zm_.y));
-            float2 B = make_float2(0.5f * (zk.y + zm_.y), -0.5f * (zk.x - zm_.x));
+            float2 A = half_spec_a(zk, zm_);
+            float2 B = half_spec_b(zk, zm_);
             if (la < g.nlines) d[g.base(la) + (long long)k * g.si] = A;
             if (la + 1 < g.nlines) d[g.base(la + 1) + (long long)k * g.si] = B;
         }

@@ -185,8 +185,8 @@ struct RStoreHalfPair {
             float2 zn = Z[k == 0 ? 0 : n - k];
             long long o = (long long)k * g.si;
             const float w = (k == 0 || 2 * k == n) ? 1.f : wpair;
-            if (c.a) c.a[o] = c_scale(make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y)), w);
-            if (c.b) c.b[o] = c_scale(make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x)), w);
+            if (c.a) c.a[o] = c_scale(half_spec_a(zk, zn), w);
+            if (c.b) c.b[o] = c_scale(half_spec_b(zk, zn), w);
         }
     }
 };
@@ -215,8 +215,8 @@ struct RStoreFullPair {
             float2 zk = Z[k];
             float2 zn = Z[k == 0 ? 0 : n - k];
             long long o = (long long)k * g.si;
-            if (c.a) c.a[o] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-            if (c.b) c.b[o] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+            if (c.a) c.a[o] = half_spec_a(zk, zn);
+            if (c.b) c.b[o] = half_spec_b(zk, zn);
         }
     }
 };
