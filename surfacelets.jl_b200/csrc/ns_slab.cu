@@ -523,6 +523,8 @@ __global__ void __launch_bounds__(kSlabThreads, MINB) ns_slab_inv_kernel(SlabArg
                 }
             }
         }
+        // the row phase's accesses to every column ahead of the next unit's copies into them
+        if (requested) fence_proxy_async();
         __syncthreads();
         // 3. C2R along axis 1, columns 2l and 2l+1 as one complex line; rows k1 >= nk1 are zero
         {
